@@ -1,0 +1,126 @@
+/*
+ * lib_ipm.so / lib_ipm_double.so -- inverse polygon mapping, C ABI.
+ *
+ * Drop-in for the reference's src/lib_ipm.cu (weisluke/irs): same symbol names
+ * and signatures, so microlensing/IPM/lib_ipm.py and lib_ipm_double.py bind
+ * them unchanged. IPM_DTYPE is float for lib_ipm.so and double for
+ * lib_ipm_double.so (src/lib_ipm.cu:4-10). The object handle is opaque.
+ *
+ * Pointers returned by get_stars / get_pixels* are host memory owned by the
+ * object, valid until the next run() or destroy() on that object (the
+ * reference returns managed memory valid until the next run()).
+ * run() and save() return false after printing the reason to stderr.
+ */
+#ifndef IRS_B200_LIB_IPM_H
+#define IRS_B200_LIB_IPM_H
+#include <stdbool.h>
+
+#ifndef IPM_DTYPE
+#define IPM_DTYPE float
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void IPMHandle;
+
+/* src/lib_ipm.cu:15 */
+IPMHandle* init(void);
+
+/* setters, src/lib_ipm.cu:17-42 */
+void set_kappa_tot(IPMHandle* self, IPM_DTYPE val);
+void set_shear(IPMHandle* self, IPM_DTYPE val);
+void set_kappa_star(IPMHandle* self, IPM_DTYPE val);
+void set_theta_star(IPMHandle* self, IPM_DTYPE val);
+void set_mass_function(IPMHandle* self, const char* val);
+void set_m_solar(IPMHandle* self, IPM_DTYPE val);
+void set_m_lower(IPMHandle* self, IPM_DTYPE val);
+void set_m_upper(IPMHandle* self, IPM_DTYPE val);
+void set_light_loss(IPMHandle* self, IPM_DTYPE val);
+void set_rectangular(IPMHandle* self, int val);
+void set_approx(IPMHandle* self, int val);
+void set_safety_scale(IPMHandle* self, IPM_DTYPE val);
+void set_starfile(IPMHandle* self, const char* val);
+void set_center_y1(IPMHandle* self, IPM_DTYPE val);
+void set_center_y2(IPMHandle* self, IPM_DTYPE val);
+void set_half_length_y1(IPMHandle* self, IPM_DTYPE val);
+void set_half_length_y2(IPMHandle* self, IPM_DTYPE val);
+void set_num_pixels_y1(IPMHandle* self, int val);
+void set_num_pixels_y2(IPMHandle* self, int val);
+void set_num_rays_y(IPMHandle* self, int val);
+void set_random_seed(IPMHandle* self, int val);
+void set_write_stars(IPMHandle* self, int val);
+void set_write_maps(IPMHandle* self, int val);
+void set_write_parities(IPMHandle* self, int val);
+void set_write_histograms(IPMHandle* self, int val);
+void set_outfile_prefix(IPMHandle* self, const char* val);
+
+/* getters, src/lib_ipm.cu:44-69 */
+IPM_DTYPE get_kappa_tot(IPMHandle* self);
+IPM_DTYPE get_shear(IPMHandle* self);
+IPM_DTYPE get_kappa_star(IPMHandle* self);
+IPM_DTYPE get_theta_star(IPMHandle* self);
+const char* get_mass_function(IPMHandle* self);
+IPM_DTYPE get_m_solar(IPMHandle* self);
+IPM_DTYPE get_m_lower(IPMHandle* self);
+IPM_DTYPE get_m_upper(IPMHandle* self);
+IPM_DTYPE get_light_loss(IPMHandle* self);
+int get_rectangular(IPMHandle* self);
+int get_approx(IPMHandle* self);
+IPM_DTYPE get_safety_scale(IPMHandle* self);
+const char* get_starfile(IPMHandle* self);
+IPM_DTYPE get_center_y1(IPMHandle* self);
+IPM_DTYPE get_center_y2(IPMHandle* self);
+IPM_DTYPE get_half_length_y1(IPMHandle* self);
+IPM_DTYPE get_half_length_y2(IPMHandle* self);
+int get_num_pixels_y1(IPMHandle* self);
+int get_num_pixels_y2(IPMHandle* self);
+int get_num_rays_y(IPMHandle* self);
+int get_random_seed(IPMHandle* self);
+int get_write_stars(IPMHandle* self);
+int get_write_maps(IPMHandle* self);
+int get_write_parities(IPMHandle* self);
+int get_write_histograms(IPMHandle* self);
+const char* get_outfile_prefix(IPMHandle* self);
+
+/* results, src/lib_ipm.cu:71-78 */
+int get_num_stars(IPMHandle* self);
+IPM_DTYPE get_corner_x1(IPMHandle* self);
+IPM_DTYPE get_corner_x2(IPMHandle* self);
+IPM_DTYPE* get_stars(IPMHandle* self);          /* (x1, x2, m) x num_stars, tree order */
+IPM_DTYPE* get_pixels(IPMHandle* self);         /* [num_pixels_y2][num_pixels_y1] magnification */
+IPM_DTYPE* get_pixels_minima(IPMHandle* self);  /* NULL unless write_parities */
+IPM_DTYPE* get_pixels_saddles(IPMHandle* self); /* NULL unless write_parities */
+double get_t_shoot_cells(IPMHandle* self);      /* seconds */
+
+/* src/lib_ipm.cu:80-81 */
+bool run(IPMHandle* self, int verbose);
+bool save(IPMHandle* self, int verbose);
+
+/* ---- extensions (no counterpart in the reference ABI) ---- */
+void destroy(IPMHandle* self);                       /* the reference never frees its objects */
+void set_expansion_order(IPMHandle* self, int order); /* 0: reference formula (ipm.cuh:848); 3..31 fixed */
+int get_expansion_order(IPMHandle* self);             /* order used by the last run */
+void set_precision(IPMHandle* self, int mode);        /* 0 default, 1 FP64 plain form, 2 FP32 form */
+int get_precision(IPMHandle* self);
+/* star field from memory: n records (x1, x2, m), with a star file's shape, corner and theta_star */
+void set_stars(IPMHandle* self, const IPM_DTYPE* xym, int n, int rectangular, IPM_DTYPE corner_x1,
+               IPM_DTYPE corner_x2, IPM_DTYPE theta);
+double get_t_pipeline(IPMHandle* self);               /* seconds: tree + expansions + shoot */
+bool rerun(IPMHandle* self, int repeats, double* seconds); /* re-run tree+expansions+shoot on the resident stars */
+bool derive(IPMHandle* self);                          /* validate + derived parameters, no GPU work */
+double get_value(IPMHandle* self, const char* name);   /* derived / run-time value by name, NaN if unknown */
+/* diagnostics: copies of internal device state */
+int get_tree_num_nodes(IPMHandle* self);
+bool copy_tree(IPMHandle* self, int* ints, double* geom, int* nbr, int* sil, int* dil);
+bool copy_coeffs(IPMHandle* self, double* mult, double* loc);
+long long get_num_vertices(IPMHandle* self);
+bool copy_vertices(IPMHandle* self, double* out);
+bool copy_fixed_maps(IPMHandle* self, unsigned long long* total, unsigned long long* minima,
+                     unsigned long long* saddles);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

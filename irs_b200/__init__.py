@@ -1,0 +1,9 @@
+"""irs_b200: B200-native microlensing magnification maps (IRS and IPM).
+
+The compute path is hand-written CUDA for sm_100a behind a C ABI
+(include/lib_ipm.h, include/lib_irs.h); this package holds the ctypes
+interface. Build the libraries with `python -m irs_b200.build`.
+"""
+from .mapmaker import IPM, IRS  # noqa: F401
+
+__all__ = ["IPM", "IRS"]

@@ -1,0 +1,195 @@
+// extern "C" entry points. One translation unit, compiled four times:
+//   -DIRSB_DOUBLE=0 -DIRSB_IRS=0  -> lib_ipm.so         (IPM, float)
+//   -DIRSB_DOUBLE=1 -DIRSB_IRS=0  -> lib_ipm_double.so  (IPM, double)
+//   -DIRSB_DOUBLE=0 -DIRSB_IRS=1  -> lib_irs.so         (IRS, float)
+//   -DIRSB_DOUBLE=1 -DIRSB_IRS=1  -> lib_irs_double.so  (IRS, double)
+// The IPM libraries export the symbol set of the reference's src/lib_ipm.cu
+// (lines 15-81) with the same signatures, so its ctypes wrapper
+// (microlensing/IPM/lib_ipm.py) binds them unchanged. The IRS libraries use
+// the same conventions (the reference has no IRS library). Declarations and
+// the list of extensions are in include/lib_ipm.h and include/lib_irs.h.
+#include "engine.cuh"
+
+#include <cstring>
+#include <limits>
+
+#ifndef IRSB_DOUBLE
+#define IRSB_DOUBLE 0
+#endif
+#ifndef IRSB_IRS
+#define IRSB_IRS 0
+#endif
+
+#if IRSB_DOUBLE
+using dtype = double;
+#else
+using dtype = float;
+#endif
+using Obj = irsb::MapMaker<dtype, bool(IRSB_IRS)>;
+using Pix = Obj::Pix;
+
+#define SETTER(name, field) \
+  void set_##name(Obj* self, dtype val) { self->prm.field = val; } \
+  dtype get_##name(Obj* self) { return self->prm.field; }
+#define ISETTER(name, field) \
+  void set_##name(Obj* self, int val) { self->prm.field = val; } \
+  int get_##name(Obj* self) { return self->prm.field; }
+#define SSETTER(name, field) \
+  void set_##name(Obj* self, const char* val) { self->prm.field = val ? val : ""; } \
+  const char* get_##name(Obj* self) { return self->prm.field.c_str(); }
+
+extern "C" {
+
+Obj* init() { return new Obj(); }
+
+SETTER(kappa_tot, kappa_tot)
+SETTER(shear, shear)
+SETTER(kappa_star, kappa_star)
+SETTER(theta_star, theta_star)
+SSETTER(mass_function, mass_function)
+SETTER(m_solar, m_solar)
+SETTER(m_lower, m_lower)
+SETTER(m_upper, m_upper)
+SETTER(light_loss, light_loss)
+ISETTER(rectangular, rectangular)
+ISETTER(approx, approx)
+SETTER(safety_scale, safety_scale)
+SSETTER(starfile, starfile)
+SETTER(center_y1, center_y.re)
+SETTER(center_y2, center_y.im)
+SETTER(half_length_y1, half_length_y.re)
+SETTER(half_length_y2, half_length_y.im)
+ISETTER(num_pixels_y1, num_pixels_y.re)
+ISETTER(num_pixels_y2, num_pixels_y.im)
+ISETTER(num_rays_y, num_rays_y)
+ISETTER(random_seed, random_seed)
+ISETTER(write_stars, write_stars)
+ISETTER(write_maps, write_maps)
+ISETTER(write_parities, write_parities)
+ISETTER(write_histograms, write_histograms)
+SSETTER(outfile_prefix, outfile_prefix)
+
+int get_num_stars(Obj* self) { return self->prm.num_stars; }
+dtype get_corner_x1(Obj* self) { return self->corner_out().re; }
+dtype get_corner_x2(Obj* self) { return self->corner_out().im; }
+dtype* get_stars(Obj* self) { return self->stars_ptr(); }
+Pix* get_pixels(Obj* self) { return self->pixels(); }
+Pix* get_pixels_minima(Obj* self) { return self->pixels_minima(); }
+Pix* get_pixels_saddles(Obj* self) { return self->pixels_saddles(); }
+#if IRSB_IRS
+double get_t_shoot_rays(Obj* self) { return self->t_shoot; }
+unsigned long long get_num_rays_shot(Obj* self) { return self->num_rays_shot; }
+unsigned long long get_num_rays_received(Obj* self) { return self->num_rays_received; }
+#else
+double get_t_shoot_cells(Obj* self) { return self->t_shoot; }
+#endif
+
+bool run(Obj* self, int verbose) { return self->run(verbose); }
+bool save(Obj* self, int verbose) { return self->save(verbose); }
+
+// ---------------------------------------------------------------- extensions
+void destroy(Obj* self) { delete self; }
+
+// 0: expansion order from the reference formula (default); 3..31: fixed order
+void set_expansion_order(Obj* self, int order) { self->prm.expansion_order_override = order; }
+int get_expansion_order(Obj* self) { return self->prm.expansion_order; }
+
+// 0: default form (FP32 for float libraries, FP64 for double ones), 1: FP64, 2: FP32
+void set_precision(Obj* self, int mode) { self->precision = mode; }
+int get_precision(Obj* self) { return self->precision; }
+
+// Star field from host memory: n records of (x1, x2, mass), with the field
+// shape, corner and theta_star of a star file. Used instead of generating
+// stars; the array is copied.
+void set_stars(Obj* self, const dtype* xym, int n, int rectangular, dtype corner_x1, dtype corner_x2, dtype theta) {
+  if (!xym || n <= 0) {
+    self->use_host_stars = false;
+    self->host_stars.clear();
+    return;
+  }
+  self->host_stars.resize(n);
+  std::memcpy(self->host_stars.data(), xym, size_t(n) * 3 * sizeof(dtype));
+  self->host_rect = rectangular;
+  self->host_corner = irsb::mk<dtype>(corner_x1, corner_x2);
+  self->host_theta = theta;
+  self->use_host_stars = true;
+}
+
+double get_t_pipeline(Obj* self) { return self->t_pipeline; }
+
+// Re-runs tree, expansions and shoot `repeats` times on the star field of the
+// last run() (device resident); *seconds receives the summed device time.
+bool rerun(Obj* self, int repeats, double* seconds) { return self->rerun(repeats, seconds); }
+
+// Checks the inputs and computes the derived parameters only (no GPU work).
+bool derive(Obj* self) {
+  irsb::Params<dtype> p = self->prm;
+  if (!irsb::check_input_params(p)) return false;
+  std::vector<irsb::StarRec<dtype>> st;
+  if (!irsb::derive_params<dtype>(p, st)) return false;
+  self->prm = p;
+  return true;
+}
+
+// Derived or run-time quantity by name; NaN for an unknown name.
+double get_value(Obj* self, const char* name) {
+  const auto& p = self->prm;
+  std::string n = name ? name : "";
+  if (n == "mu_ave") return p.mu_ave;
+  if (n == "num_rays_x") return p.num_rays_x;
+  if (n == "ray_half_sep_1") return p.ray_half_sep.re;
+  if (n == "ray_half_sep_2") return p.ray_half_sep.im;
+  if (n == "half_length_x1") return p.half_length_x.re;
+  if (n == "half_length_x2") return p.half_length_x.im;
+  if (n == "center_x1") return p.center_x.re;
+  if (n == "center_x2") return p.center_x.im;
+  if (n == "num_ray_threads_1") return p.num_ray_threads.re;
+  if (n == "num_ray_threads_2") return p.num_ray_threads.im;
+  if (n == "corner_x1") return p.corner.re;
+  if (n == "corner_x2") return p.corner.im;
+  if (n == "rad") return irsb::cabs_(p.corner);
+  if (n == "num_stars") return p.num_stars;
+  if (n == "alpha_error") return p.alpha_error;
+  if (n == "taylor_smooth") return p.taylor_smooth;
+  if (n == "mean_mass") return p.mean_mass;
+  if (n == "mean_mass2") return p.mean_mass2;
+  if (n == "mean_mass2_ln_mass") return p.mean_mass2_ln_mass;
+  if (n == "m_lower") return p.m_lower;
+  if (n == "m_upper") return p.m_upper;
+  if (n == "kappa_star_actual") return p.kappa_star_actual;
+  if (n == "m_lower_actual") return p.m_lower_actual;
+  if (n == "m_upper_actual") return p.m_upper_actual;
+  if (n == "mean_mass_actual") return p.mean_mass_actual;
+  if (n == "mean_mass2_actual") return p.mean_mass2_actual;
+  if (n == "mean_mass2_ln_mass_actual") return p.mean_mass2_ln_mass_actual;
+  if (n == "root_half_length") return p.root_half_length;
+  if (n == "expansion_order") return p.expansion_order;
+  if (n == "tree_levels") return p.tree_levels;
+  if (n == "random_seed") return p.random_seed;
+  if (n == "num_leaves") return self->num_leaves;
+  if (n == "num_tiles") return double(self->num_tiles);
+  if (n == "t_shoot") return self->t_shoot;
+  if (n == "t_pipeline") return self->t_pipeline;
+  if (n == "t_lattice") return self->t_lattice;
+  if (n == "t_deposit") return self->t_deposit;
+  if (n == "mean_near") return self->mean_near;
+  if (n == "launches") return double(self->launches);
+  if (n == "num_lattice_points") return double(self->num_tiles >= 0 ? 1 : 0) *
+      (IRSB_IRS ? double(p.num_ray_threads.re) * p.num_ray_threads.im
+                : double(p.num_ray_threads.re + 1) * (p.num_ray_threads.im + 1));
+  return std::numeric_limits<double>::quiet_NaN();
+}
+
+// ---------------------------------------------------------------- diagnostics
+int get_tree_num_nodes(Obj* self) { return self->tree_num_nodes(); }
+bool copy_tree(Obj* self, int* ints, double* geom, int* nbr, int* sil, int* dil) {
+  return self->copy_tree(ints, geom, nbr, sil, dil);
+}
+bool copy_coeffs(Obj* self, double* mult, double* loc) { return self->copy_coeffs(mult, loc); }
+long long get_num_vertices(Obj* self) { return self->num_vertices(); }
+bool copy_vertices(Obj* self, double* out) { return self->copy_vertices(out); }
+bool copy_fixed_maps(Obj* self, unsigned long long* total, unsigned long long* mn, unsigned long long* sd) {
+  return self->copy_fixed_maps(total, mn, sd);
+}
+
+}  // extern "C"

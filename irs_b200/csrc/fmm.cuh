@@ -1,0 +1,228 @@
+// Multipole / local expansion coefficients of the quadtree, in FP64.
+//
+// Formulas of the reference's fmm.cuh (coefficients in units of the node half
+// length):
+//   P2M  a_0 = sum m_i, a_k = -sum m_i ((z_i - c)/hl)^k / k          fmm.cuh:21-49
+//   M2M  dz = (c_child - c_parent)/hl_child,
+//        b_l = (sum_k a_k C(l-1,k-1) / dz^k - a_0/l) * (dz/2)^l       fmm.cuh:109-139
+//   L2L  dz = (c - c_parent)/hl_parent,
+//        d_l = sum_{k>=1} c_k C(k,l) dz^k / (2 dz)^l                 fmm.cuh:204-223
+//   M2L  dz = (c_from - c_to)/hl_from,
+//        c_0 = sum_k b_k/(-dz)^k + b_0 log(-dz) + b_0 log(hl_from),
+//        c_l = (sum_k b_k C(l+k-1,k-1)/(-dz)^k - b_0/l) / dz^l       fmm.cuh:281-322
+//   P2L  dz = (z_i - c_to)/hl_to,
+//        c_0 = sum m_i (log(-dz) + log(hl_to)), c_l = -sum m_i/(l dz^l) fmm.cuh:387-413
+// evaluated with the reference's Horner ordering. Level schedule as
+// include/ipm.cuh:874-901: P2M+M2M bottom-up, then L2L, M2L, P2L top-down from
+// level 2. The reference builds an int binomial table, which overflows beyond
+// order ~17 (binomial_coefficients.cuh:11-44); this table is int64, exact up to
+// row 62, and is used as double.
+//
+// Layout: coefficients of node k, order l at [k * (p + 1) + l] as double2.
+// Kernel shape: one warp per node, lane l computes order l (p <= 31).
+#pragma once
+#include "common.cuh"
+#include "devutil.cuh"
+#include "tree.cuh"
+
+#include <vector>
+
+namespace irsb {
+
+__device__ __forceinline__ cplx<double> ld2(const double2* p) {
+  double2 v = *p;
+  return mk<double>(v.x, v.y);
+}
+__device__ __forceinline__ void st2(double2* p, cplx<double> c) { *p = make_double2(c.re, c.im); }
+
+inline std::vector<double> binomial_table(int nmax) {
+  // row n starts at n(n+1)/2
+  std::vector<long long> t((nmax + 1) * (nmax + 2) / 2);
+  for (int n = 0; n <= nmax; n++) {
+    int r = n * (n + 1) / 2, pr = (n - 1) * n / 2;
+    for (int i = 0; i <= n; i++) t[r + i] = (i == 0 || i == n) ? 1 : t[pr + i - 1] + t[pr + i];
+  }
+  return std::vector<double>(t.begin(), t.end());
+}
+__device__ __forceinline__ double binom(const double* tab, int n, int k) {
+  if (n < k || k < 0) return 0.0;
+  return tab[n * (n + 1) / 2 + k];
+}
+
+template <typename T>
+__global__ void fmm_p2m(int beg, int end, int p, const T* __restrict__ cx, const T* __restrict__ cy,
+                        const T* __restrict__ hl, const int* __restrict__ child0, const int* __restrict__ sbeg,
+                        const int* __restrict__ scnt, const StarRec<T>* __restrict__ stars, double2* mult) {
+  int lane = threadIdx.x & 31;
+  int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int k = beg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < end; k += warps) {
+    if (child0[k] >= 0 || scnt[k] == 0) continue;
+    if (lane > p) continue;
+    double ccx = cx[k], ccy = cy[k], h = hl[k];
+    int b = sbeg[k], n = scnt[k];
+    cplx<double> r = mk(0.0, 0.0);
+    for (int i = 0; i < n; i++) {
+      StarRec<T> s = stars[b + i];
+      if (lane == 0) {
+        r.re += double(s.m);
+      } else {
+        cplx<double> d = mk((double(s.x) - ccx) / h, (double(s.y) - ccy) / h);
+        r = csub(r, cscale(cpowi(d, lane), double(s.m)));
+      }
+    }
+    if (lane > 0) r = cdivr(r, double(lane));
+    st2(&mult[(size_t)k * (p + 1) + lane], r);
+  }
+}
+
+// Parent multipoles from its 4 children (internal nodes of one level).
+template <typename T>
+__global__ void fmm_m2m(int beg, int end, int p, const T* __restrict__ cx, const T* __restrict__ cy,
+                        const T* __restrict__ hl, const int* __restrict__ child0, const double* __restrict__ btab,
+                        double2* mult) {
+  int lane = threadIdx.x & 31;
+  int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int k = beg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < end; k += warps) {
+    int c0 = child0[k];
+    if (c0 < 0 || lane > p) continue;
+    cplx<double> acc = mk(0.0, 0.0);
+    for (int j = 0; j < 4; j++) {
+      int c = c0 + j;
+      const double2* a = mult + (size_t)c * (p + 1);
+      cplx<double> r;
+      if (lane == 0) {
+        r = ld2(a);
+      } else {
+        double hc = hl[c];
+        cplx<double> dz = mk((double(cx[c]) - double(cx[k])) / hc, (double(cy[c]) - double(cy[k])) / hc);
+        r = mk(0.0, 0.0);
+        for (int i = p; i >= 1; i--) {
+          r = cadd(r, cscale(ld2(a + i), binom(btab, lane - 1, i - 1)));
+          r = cdiv(r, dz);
+        }
+        r = csub(r, cdivr(ld2(a), double(lane)));
+        r = cmul(r, cpowi(dz, lane));
+        r = cdivr(r, double(1u << lane));
+      }
+      acc = cadd(acc, r);
+    }
+    st2(&mult[(size_t)k * (p + 1) + lane], acc);
+  }
+}
+
+// Local coefficients of the nodes of one level (>= 2): L2L from the parent,
+// then M2L over the same-level interaction list, then P2L over the
+// different-level list, accumulated in that order.
+template <typename T>
+__global__ void fmm_local(int beg, int end, int p, const T* __restrict__ cx, const T* __restrict__ cy,
+                          const T* __restrict__ hl, const int* __restrict__ parent, const int* __restrict__ sbeg,
+                          const int* __restrict__ scnt, const int* __restrict__ sil, const int* __restrict__ n_sil,
+                          const int* __restrict__ dil, const int* __restrict__ n_dil,
+                          const StarRec<T>* __restrict__ stars, const double* __restrict__ btab,
+                          const double2* __restrict__ mult, double2* loc) {
+  int lane = threadIdx.x & 31;
+  int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int k = beg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < end; k += warps) {
+    if (lane > p) continue;
+    const double ccx = cx[k], ccy = cy[k], h = hl[k];
+    // L2L
+    int pa = parent[k];
+    const double2* cp = loc + (size_t)pa * (p + 1);
+    double hp = hl[pa];
+    cplx<double> dz = mk((ccx - double(cx[pa])) / hp, (ccy - double(cy[pa])) / hp);
+    cplx<double> r = mk(0.0, 0.0);
+    for (int i = p; i >= 1; i--) {
+      r = cadd(r, cscale(ld2(cp + i), binom(btab, i, lane)));
+      r = cmul(r, dz);
+    }
+    r = cdiv(r, cpowi(dz, lane));
+    r = cdivr(r, double(1u << lane));
+    cplx<double> acc = r;
+    // M2L
+    int ns = n_sil[k];
+    for (int j = 0; j < ns; j++) {
+      int f = sil[k * kMaxSameLevelIL + j];
+      const double2* b = mult + (size_t)f * (p + 1);
+      double hf = hl[f];
+      cplx<double> d = mk((double(cx[f]) - ccx) / hf, (double(cy[f]) - ccy) / hf);
+      cplx<double> md = cneg(d);
+      cplx<double> t = mk(0.0, 0.0);
+      if (lane == 0) {
+        for (int i = p; i >= 1; i--) {
+          t = cadd(t, ld2(b + i));
+          t = cdiv(t, md);
+        }
+        cplx<double> b0 = ld2(b);
+        t = cadd(t, cmul(b0, clog_(md)));
+        t = cadd(t, cscale(b0, log(hf)));
+      } else {
+        for (int i = p; i >= 1; i--) {
+          t = cadd(t, cscale(ld2(b + i), binom(btab, lane + i - 1, i - 1)));
+          t = cdiv(t, md);
+        }
+        t = csub(t, cdivr(ld2(b), double(lane)));
+        t = cdiv(t, cpowi(d, lane));
+      }
+      acc = cadd(acc, t);
+    }
+    // P2L
+    int nd = n_dil[k];
+    for (int j = 0; j < nd; j++) {
+      int f = dil[k * kMaxDiffLevelIL + j];
+      int sb = sbeg[f], sn = scnt[f];
+      cplx<double> t = mk(0.0, 0.0);
+      for (int i = 0; i < sn; i++) {
+        StarRec<T> s = stars[sb + i];
+        cplx<double> d = mk((double(s.x) - ccx) / h, (double(s.y) - ccy) / h);
+        double m = double(s.m);
+        if (lane == 0) {
+          t = cadd(t, cscale(clog_(cneg(d)), m));
+          t.re += m * log(h);
+        } else {
+          t = csub(t, cdiv(mk(m, 0.0), cscale(cpowi(d, lane), double(lane))));
+        }
+      }
+      acc = cadd(acc, t);
+    }
+    st2(&loc[(size_t)k * (p + 1) + lane], acc);
+  }
+}
+
+struct FmmDev {
+  int p = 0;
+  DevVec<double2> mult, loc;
+  DevVec<double> btab;
+};
+
+template <typename T>
+bool compute_fmm(FmmDev& f, TreeDev<T>& t, const StarRec<T>* stars, int p, cudaStream_t s) {
+  f.p = p;
+  size_t ncoef = size_t(t.num_nodes) * (p + 1);
+  if (!f.mult.alloc_exact(ncoef) || !f.loc.alloc_exact(ncoef)) return false;
+  IRSB_CKR(cudaMemsetAsync(f.mult.p, 0, ncoef * sizeof(double2), s));
+  IRSB_CKR(cudaMemsetAsync(f.loc.p, 0, ncoef * sizeof(double2), s));
+  std::vector<double> bt = binomial_table(2 * kMaxOrder);
+  if (!f.btab.alloc_exact(bt.size())) return false;
+  IRSB_CKR(cudaMemcpyAsync(f.btab.p, bt.data(), bt.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  for (int l = t.levels; l >= 0; l--) {
+    int beg = t.level_off[l], end = t.level_off[l + 1];
+    int nw = end - beg;
+    int blocks = std::max(1, std::min(ceil_div(nw, 8), 148 * 16));
+    fmm_p2m<T><<<blocks, 256, 0, s>>>(beg, end, p, t.cx.p, t.cy.p, t.hl.p, t.child0.p, t.sbeg.p, t.scnt.p, stars,
+                                      f.mult.p);
+    IRSB_LAUNCH_CK("fmm_p2m");
+    fmm_m2m<T><<<blocks, 256, 0, s>>>(beg, end, p, t.cx.p, t.cy.p, t.hl.p, t.child0.p, f.btab.p, f.mult.p);
+    IRSB_LAUNCH_CK("fmm_m2m");
+  }
+  for (int l = 2; l <= t.levels; l++) {
+    int beg = t.level_off[l], end = t.level_off[l + 1];
+    int nw = end - beg;
+    int blocks = std::max(1, std::min(ceil_div(nw, 8), 148 * 16));
+    fmm_local<T><<<blocks, 256, 0, s>>>(beg, end, p, t.cx.p, t.cy.p, t.hl.p, t.parent.p, t.sbeg.p, t.scnt.p,
+                                        t.sil.p, t.n_sil.p, t.dil.p, t.n_dil.p, stars, f.btab.p, f.mult.p, f.loc.p);
+    IRSB_LAUNCH_CK("fmm_local");
+  }
+  return true;
+}
+
+}  // namespace irsb

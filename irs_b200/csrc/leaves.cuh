@@ -1,0 +1,205 @@
+// Per-leaf records consumed by the shooting kernels, and the partition of a
+// regular lattice (rays for IRS, cell vertices for IPM) into leaf tiles.
+//
+// A ray is evaluated with the leaf that get_nearest_node (tree_node.cuh:529-561)
+// returns for it, i.e. its near field is the leaf's own stars plus its
+// neighbours' stars (alpha_star.cuh:18-41, neighbours first) and its far field
+// is the leaf's local expansion (alpha_local.cuh:18-36). Here that lookup is
+// done once per leaf instead of once per ray: every leaf box [lox, hix) x
+// [loy, hiy) covers a rectangle of lattice indices, found by binary search on
+// the lattice coordinate formula (which is monotone in the index). The
+// rectangles are cut into TX x TY tiles; a prefix sum over leaves maps a global
+// tile number back to (leaf, tile).
+//
+// Record layout (structure of arrays over leaves, 32 slots per leaf):
+//   near64[l][s] = (x, y, m, 0)            FP64 plain path, global coordinates
+//   near32[l][s] = (x - cx, y - cy, m theta^2, 0)  FP32 path, leaf-relative
+//   coef64[l][k] = k * c_k, k = 1..p       (slot k-1)
+//   coef32[l][k] = theta^2 (k+1) c_{k+1} / hl, k = 0..p-1: conj(alpha_local) =
+//                  sum_k coef32[k] dz^k with dz = (z - c) / hl
+#pragma once
+#include "common.cuh"
+#include "devutil.cuh"
+#include "fmm.cuh"
+#include "tree.cuh"
+
+namespace irsb {
+
+constexpr int kTileX = 32;
+constexpr int kTileY = 32;
+
+struct LeafSet {
+  int n = 0;
+  DevVec<int> flag;
+  DevVec<long long> pos;
+  DevVec<int> node;
+  DevVec<double> cx, cy, hl;
+  DevVec<int> nnear;
+  DevVec<double4> near64;
+  DevVec<float4> near32;
+  DevVec<double2> coef64;
+  DevVec<float2> coef32;
+  ScanScratch scan;
+};
+
+// Lattice partition for one lattice (rays or vertices).
+struct LatticeTiles {
+  DevVec<int4> rect;  // i0, i1, j0, j1
+  DevVec<long long> tiles;
+  DevVec<long long> tile_off;  // [n + 1]
+  long long total = 0;
+  ScanScratch scan;
+};
+
+__global__ void leaf_flags(int n, const int* __restrict__ child0, int* flag) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) flag[k] = child0[k] < 0;
+}
+__global__ void leaf_compact(int n, const int* __restrict__ flag, const long long* __restrict__ pos, int* node) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    if (flag[k]) node[pos[k]] = k;
+}
+
+// One warp per leaf: gather the near field and the expansion coefficients.
+template <typename T>
+__global__ void leaf_build(int nleaves, int p, double theta, const int* __restrict__ leaf_node,
+                           const T* __restrict__ cx, const T* __restrict__ cy, const T* __restrict__ hl,
+                           const int* __restrict__ sbeg, const int* __restrict__ scnt, const int* __restrict__ nbr,
+                           const int* __restrict__ n_nbr, const StarRec<T>* __restrict__ stars,
+                           const double2* __restrict__ loc, double* lcx, double* lcy, double* lhl, int* nnear,
+                           double4* near64, float4* near32, double2* coef64, float2* coef32, int* dstat) {
+  int lane = threadIdx.x & 31;
+  int warps = (gridDim.x * blockDim.x) >> 5;
+  double th2 = theta * theta;
+  for (int l = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; l < nleaves; l += warps) {
+    int k = leaf_node[l];
+    double ccx = double(cx[k]), ccy = double(cy[k]), h = double(hl[k]);
+    if (lane == 0) {
+      lcx[l] = ccx;
+      lcy[l] = ccy;
+      lhl[l] = h;
+    }
+    // near list: neighbours in order, then the leaf itself
+    int nn = n_nbr[k];
+    int out = 0;
+    for (int j = 0; j <= nn; j++) {
+      int src = j < nn ? nbr[k * kMaxNeighbors + j] : k;
+      int b = sbeg[src], c = scnt[src];
+      for (int i = lane; i < c; i += 32) {
+        int slot = out + i;
+        if (slot < kMaxStarsDirect) {
+          StarRec<T> s = stars[b + i];
+          near64[(size_t)l * kMaxStarsDirect + slot] = make_double4(double(s.x), double(s.y), double(s.m), 0.0);
+          near32[(size_t)l * kMaxStarsDirect + slot] =
+              make_float4(float(double(s.x) - ccx), float(double(s.y) - ccy), float(double(s.m) * th2), 0.f);
+        }
+      }
+      out += c;
+    }
+    if (out > kMaxStarsDirect) {
+      if (lane == 0) atomicOr(&dstat[0], kErrNearOverflow);
+      out = kMaxStarsDirect;
+    }
+    // zero the unused slots so that any over-read is harmless
+    for (int slot = out + lane; slot < kMaxStarsDirect; slot += 32) {
+      near64[(size_t)l * kMaxStarsDirect + slot] = make_double4(0, 0, 0, 0);
+      near32[(size_t)l * kMaxStarsDirect + slot] = make_float4(0, 0, 0, 0);
+    }
+    if (lane == 0) nnear[l] = out;
+    // local expansion coefficients
+    if (lane < p) {
+      int kk = lane + 1;
+      double2 c = loc[(size_t)k * (p + 1) + kk];
+      coef64[(size_t)l * kMaxOrder + lane] = make_double2(c.x * kk, c.y * kk);
+      double s = th2 * kk / h;
+      coef32[(size_t)l * kMaxOrder + lane] = make_float2(float(c.x * s), float(c.y * s));
+    } else if (lane < kMaxOrder) {
+      coef64[(size_t)l * kMaxOrder + lane] = make_double2(0, 0);
+      coef32[(size_t)l * kMaxOrder + lane] = make_float2(0, 0);
+    }
+  }
+}
+
+// Lattice coordinate of index i: base + 2 * (rhs * i), the operation order of
+// the reference's ray positions (irs_functions.cuh:122).
+__device__ __forceinline__ double lattice_coord(double base, double rhs, long long i) {
+  return base + 2.0 * (rhs * double(i));
+}
+// first index in [0, n] with coordinate >= v
+__device__ __forceinline__ long long lattice_lower_bound(double base, double rhs, long long n, double v) {
+  long long lo = 0, hi = n;
+  while (lo < hi) {
+    long long mid = (lo + hi) >> 1;
+    if (lattice_coord(base, rhs, mid) >= v)
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  return lo;
+}
+
+__global__ void leaf_rects(int nleaves, const int* __restrict__ leaf_node, const double* __restrict__ lox,
+                           const double* __restrict__ hix, const double* __restrict__ loy,
+                           const double* __restrict__ hiy, double base_x, double base_y, double rhs_x, double rhs_y,
+                           long long nx, long long ny, int tx, int ty, int4* rect, long long* tiles) {
+  for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < nleaves; l += gridDim.x * blockDim.x) {
+    int k = leaf_node[l];
+    long long i0 = lattice_lower_bound(base_x, rhs_x, nx, lox[k]);
+    long long i1 = lattice_lower_bound(base_x, rhs_x, nx, hix[k]);
+    long long j0 = lattice_lower_bound(base_y, rhs_y, ny, loy[k]);
+    long long j1 = lattice_lower_bound(base_y, rhs_y, ny, hiy[k]);
+    rect[l] = make_int4(int(i0), int(i1), int(j0), int(j1));
+    long long ni = i1 - i0, nj = j1 - j0;
+    tiles[l] = (ni > 0 && nj > 0) ? ((ni + tx - 1) / tx) * ((nj + ty - 1) / ty) : 0;
+  }
+}
+
+template <typename T>
+bool build_leaves(LeafSet& L, TreeDev<T>& t, FmmDev& f, const StarRec<T>* stars, double theta, cudaStream_t s) {
+  int n = t.num_nodes;
+  if (!L.flag.alloc_exact(n) || !L.pos.alloc_exact(n + 1)) return false;
+  int blocks = std::max(1, std::min(ceil_div(n, 256), 148 * 8));
+  leaf_flags<<<blocks, 256, 0, s>>>(n, t.child0.p, L.flag.p);
+  if (!exclusive_scan<int>(L.flag.p, n, L.pos.p, L.scan, s)) return false;
+  long long nl = 0;
+  IRSB_CKR(cudaMemcpyAsync(&nl, L.scan.sum.p, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  IRSB_CKR(cudaStreamSynchronize(s));
+  L.n = int(nl);
+  if (!L.node.alloc_exact(L.n) || !L.cx.alloc_exact(L.n) || !L.cy.alloc_exact(L.n) || !L.hl.alloc_exact(L.n) ||
+      !L.nnear.alloc_exact(L.n) || !L.near64.alloc_exact((size_t)L.n * kMaxStarsDirect) ||
+      !L.near32.alloc_exact((size_t)L.n * kMaxStarsDirect) || !L.coef64.alloc_exact((size_t)L.n * kMaxOrder) ||
+      !L.coef32.alloc_exact((size_t)L.n * kMaxOrder))
+    return false;
+  leaf_compact<<<blocks, 256, 0, s>>>(n, L.flag.p, L.pos.p, L.node.p);
+  IRSB_LAUNCH_CK("leaf_compact");
+  IRSB_CKR(cudaMemsetAsync(t.dstat.p, 0, 2 * sizeof(int), s));
+  int lb = std::max(1, std::min(ceil_div(L.n, 8), 148 * 16));
+  leaf_build<T><<<lb, 256, 0, s>>>(L.n, f.p, theta, L.node.p, t.cx.p, t.cy.p, t.hl.p, t.sbeg.p, t.scnt.p, t.nbr.p,
+                                   t.n_nbr.p, stars, f.loc.p, L.cx.p, L.cy.p, L.hl.p, L.nnear.p, L.near64.p,
+                                   L.near32.p, L.coef64.p, L.coef32.p, t.dstat.p);
+  IRSB_LAUNCH_CK("leaf_build");
+  int st = 0;
+  IRSB_CKR(cudaMemcpyAsync(&st, t.dstat.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  IRSB_CKR(cudaStreamSynchronize(s));
+  if (st) {
+    std::fprintf(stderr, "Error. A leaf's near field holds more than %d stars.\n", kMaxStarsDirect);
+    return false;
+  }
+  return true;
+}
+
+template <typename T>
+bool build_lattice_tiles(LatticeTiles& W, const LeafSet& L, TreeDev<T>& t, double base_x, double base_y,
+                         double rhs_x, double rhs_y, long long nx, long long ny, cudaStream_t s) {
+  if (!W.rect.alloc_exact(L.n) || !W.tiles.alloc_exact(L.n) || !W.tile_off.alloc_exact(L.n + 1)) return false;
+  int blocks = std::max(1, std::min(ceil_div(L.n, 256), 148 * 8));
+  leaf_rects<<<blocks, 256, 0, s>>>(L.n, L.node.p, t.lox.p, t.hix.p, t.loy.p, t.hiy.p, base_x, base_y, rhs_x, rhs_y,
+                                    nx, ny, kTileX, kTileY, W.rect.p, W.tiles.p);
+  IRSB_LAUNCH_CK("leaf_rects");
+  if (!exclusive_scan<long long>(W.tiles.p, L.n, W.tile_off.p, W.scan, s)) return false;
+  IRSB_CKR(cudaMemcpyAsync(W.tile_off.p + L.n, W.scan.sum.p, sizeof(long long), cudaMemcpyDeviceToDevice, s));
+  IRSB_CKR(cudaMemcpyAsync(&W.total, W.scan.sum.p, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  IRSB_CKR(cudaStreamSynchronize(s));
+  return true;
+}
+
+}  // namespace irsb

@@ -1,0 +1,85 @@
+// Post-pass over the finished maps: ray totals, value ranges and histograms.
+//
+// Reference behaviour (include/ipm.cuh:950-1120, include/irs.cuh:930-1028,
+// include/array_functions.cuh:114-160): IRS histograms count pixels per ray
+// count; IPM histograms bin round(mu * 1000) and round(log10(mu) * 1000),
+// offset by the minimum bin. Ranges come from a min/max over the map; sums and
+// ranges here are integer reductions, so they are deterministic.
+#pragma once
+#include "common.cuh"
+#include "devutil.cuh"
+
+#include <type_traits>
+
+namespace irsb {
+
+// Total of an int map (num_rays_received, include/irs.cuh:934-935).
+__global__ void sum_int_map(const int* __restrict__ v, long long n, unsigned long long* out) {
+  unsigned long long s = 0;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    s += (unsigned long long)v[k];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
+// min / max of non-negative values through their ordered integer encodings.
+template <typename V>
+struct OrderedKey;
+template <>
+struct OrderedKey<int> {
+  using K = int;
+  static __device__ __forceinline__ K enc(int v) { return v; }
+};
+template <>
+struct OrderedKey<float> {
+  using K = int;
+  static __device__ __forceinline__ K enc(float v) { return __float_as_int(v); }
+};
+template <>
+struct OrderedKey<double> {
+  using K = long long;
+  static __device__ __forceinline__ K enc(double v) { return __double_as_longlong(v); }
+};
+
+template <typename V>
+__global__ void minmax_nonneg(const V* __restrict__ v, long long n, typename OrderedKey<V>::K* out) {
+  using K = typename OrderedKey<V>::K;
+  K lo = OrderedKey<V>::enc(v[0]), hi = lo;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    K e = OrderedKey<V>::enc(v[k]);
+    lo = e < lo ? e : lo;
+    hi = e > hi ? e : hi;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    K a = __shfl_down_sync(0xffffffffu, lo, o), b = __shfl_down_sync(0xffffffffu, hi, o);
+    lo = a < lo ? a : lo;
+    hi = b > hi ? b : hi;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&out[0], lo);
+    atomicMax(&out[1], hi);
+  }
+}
+
+// histogram[round(v * factor - hmin)]++ ; log form uses log10(v). Values whose
+// bin falls outside [0, len) (log10 of an empty pixel) are not counted.
+template <typename V>
+__global__ void histogram_map(const V* __restrict__ v, long long n, int hmin, int len, int factor, int use_log,
+                              int* __restrict__ hist) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    double x;
+    if constexpr (std::is_floating_point<V>::value) {
+      if (use_log) {
+        V lv = log10(v[k]);
+        x = round(double(V(lv * factor - hmin)));
+      } else {
+        x = round(1.0 * v[k] * factor - hmin);
+      }
+    } else {
+      x = round(1.0 * v[k] * factor - hmin);
+    }
+    if (x >= 0 && x < len) atomicAdd(&hist[(long long)x], 1);
+  }
+}
+
+}  // namespace irsb

@@ -1,0 +1,366 @@
+// Lens-equation kernels over a regular lattice, tiled by quadtree leaf.
+//
+// Per lattice point z the source position is (complex_image_to_source,
+// irs_functions.cuh:33-45 / ipm_functions.cuh:34-46)
+//     w = (1 - kappa) z + gamma conj(z) - alpha_star - alpha_local - alpha_smooth
+// with alpha_star the leaf's near-field direct sum, alpha_local the Horner
+// evaluation of the leaf's local expansion and alpha_smooth the smooth sheet.
+//
+// Two arithmetic forms:
+//   * shoot_f64 -- the plain uniform FP64 form. Global coordinates and the
+//     reference's operation order for the ray position, the far-field Horner
+//     loop and the source-to-pixel conversion (point_to_pixel,
+//     array_functions.cuh:70-75).
+//   * shoot_f32 -- the FP32 form. Coordinates are taken relative to the leaf
+//     centre; the near-field sum runs in FP32 with blocked two-sum
+//     compensation (naive partial sums of 4 stars folded into a compensated
+//     accumulator); the far field is an FP32 Horner evaluation of coefficients
+//     built in FP64; the linear part of the lens equation is applied at the
+//     leaf centre in FP64 and the final cell-local -> global pixel conversion
+//     is FP64.
+//
+// Work distribution: a CTA takes one (leaf, 32x32 tile) work item at a time
+// (grid-stride over the global tile list), stages the leaf's <= 32 near stars
+// and <= 31 coefficients in shared memory, and every lane reads them as
+// warp-wide broadcasts. Each thread evaluates 4 lattice points (rows ty,
+// ty+8, ty+16, ty+24 of the tile) against each staged star, so one
+// shared-memory read feeds 4 evaluations.
+//
+// Outputs: IRS adds one count per ray to the int32 map with the reference's
+// clamp and row flip (irs_functions.cuh:147-198); the IPM vertex mode writes
+// the vertex's source position in pixel units with the row axis flipped
+// (ipm_functions.cuh:159-165) for the deposition pass.
+#pragma once
+#include "common.cuh"
+#include "leaves.cuh"
+#include "smooth.cuh"
+
+namespace irsb {
+
+constexpr int kShootThreads = 256;
+constexpr int kRaysPerThread = kTileY / (kShootThreads / kTileX);  // 4
+
+struct ShootParams {
+  double kappa, gamma, kstar, theta2, inv_pi;
+  int rect, approx, taylor_smooth, p;
+  double corner_re, corner_im;
+  double cy_re, cy_im;    // centre of the source region
+  double hly_re, hly_im;  // half length of the source region
+  int npx, npy;
+  double base_x, base_y;  // lattice coordinate of index 0
+  double rhs_x, rhs_y;    // half spacing of the lattice
+  long long nx, ny;       // lattice extent
+};
+
+struct LeafPtrs {
+  const double* cx;
+  const double* cy;
+  const double* hl;
+  const int* nnear;
+  const double4* near64;
+  const float4* near32;
+  const double2* coef64;
+  const float2* coef32;
+  const int4* rect;
+  const long long* tile_off;
+  int nleaves;
+};
+
+__device__ __forceinline__ int find_leaf(const long long* __restrict__ off, int n, long long t) {
+  int lo = 0, hi = n;  // off[lo] <= t < off[hi]
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (off[mid] <= t)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+struct TileInfo {
+  int leaf, i0, j0, ni, nj;
+};
+
+__device__ __forceinline__ TileInfo tile_info(const LeafPtrs& lp, long long t) {
+  TileInfo ti;
+  ti.leaf = find_leaf(lp.tile_off, lp.nleaves, t);
+  int4 r = lp.rect[ti.leaf];
+  long long local = t - lp.tile_off[ti.leaf];
+  int ntx = (r.y - r.x + kTileX - 1) / kTileX;
+  int tj = int(local / ntx), tix = int(local % ntx);
+  ti.i0 = r.x + tix * kTileX;
+  ti.j0 = r.z + tj * kTileY;
+  ti.ni = min(kTileX, r.y - ti.i0);
+  ti.nj = min(kTileY, r.w - ti.j0);
+  return ti;
+}
+
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// Adds one ray count with the reference's clamp and row flip; (px, py) are the
+// source position in pixel units (unflipped).
+__device__ __forceinline__ void irs_deposit(double px, double py, int npx, int npy, int* __restrict__ pix,
+                                            int* __restrict__ pmin, int* __restrict__ psad, bool parity_min,
+                                            bool parities) {
+  int ix = int(px), iy = int(py);
+  if (ix == npx) ix--;
+  if (iy == npy) iy--;
+  long long idx = (long long)(npy - 1 - iy) * npx + ix;
+  if (parities) atomicAdd(parity_min ? &pmin[idx] : &psad[idx], 1);
+  atomicAdd(&pix[idx], 1);
+}
+
+// ----------------------------------------------------------------- FP64 form
+template <bool VERT, bool PAR>
+__global__ void __launch_bounds__(kShootThreads) shoot_f64(ShootParams sp, LeafPtrs lp, long long total_tiles,
+                                                           int* __restrict__ pix, int* __restrict__ pmin,
+                                                           int* __restrict__ psad, double2* __restrict__ verts) {
+  __shared__ double4 s_near[kMaxStarsDirect];
+  __shared__ double2 s_coef[kMaxOrder];
+  const int tx = threadIdx.x & (kTileX - 1), ty = threadIdx.x / kTileX;
+  const cplx<double> corner = mk(sp.corner_re, sp.corner_im);
+  for (long long t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+    TileInfo ti = tile_info(lp, t);
+    const int nn = lp.nnear[ti.leaf];
+    if (threadIdx.x < kMaxStarsDirect) s_near[threadIdx.x] = lp.near64[(size_t)ti.leaf * kMaxStarsDirect + threadIdx.x];
+    if (threadIdx.x >= 64 && threadIdx.x < 64 + kMaxOrder)
+      s_coef[threadIdx.x - 64] = lp.coef64[(size_t)ti.leaf * kMaxOrder + threadIdx.x - 64];
+    const double lcx = lp.cx[ti.leaf], lcy = lp.cy[ti.leaf], lhl = lp.hl[ti.leaf];
+    __syncthreads();
+    if (tx < ti.ni) {
+      const long long i = ti.i0 + tx;
+      const double x = sp.base_x + 2.0 * (sp.rhs_x * double(i));
+#pragma unroll 1
+      for (int r = 0; r < kRaysPerThread; r++) {
+        int jj = ty + r * (kShootThreads / kTileX);
+        if (jj >= ti.nj) break;
+        const long long j = ti.j0 + jj;
+        const double y = sp.base_y + 2.0 * (sp.rhs_y * double(j));
+        // near field: sum m / (z - z_i)
+        double ar = 0.0, ai = 0.0, dr = 0.0, di = 0.0;
+        for (int s = 0; s < nn; s++) {
+          double4 st = s_near[s];
+          double ex = x - st.x, ey = y - st.y;
+          double inv = 1.0 / (ex * ex + ey * ey);
+          double q = st.z * inv;
+          ar += q * ex;
+          ai -= q * ey;
+          if (PAR) {  // m / (z - z_i)^2 = m conj(d)^2 / |d|^4
+            double t2 = q * inv;
+            dr += t2 * (ex * ex - ey * ey);
+            di -= t2 * (2.0 * ex * ey);
+          }
+        }
+        cplx<double> a_star = mk(ar * sp.theta2, -(ai * sp.theta2));
+        // far field: Horner in dz = (z - c) / hl
+        cplx<double> dz = mk((x - lcx) / lhl, (y - lcy) / lhl);
+        cplx<double> A = mk(0.0, 0.0), Ad = mk(0.0, 0.0);
+        for (int k = sp.p; k >= 1; k--) {
+          if (PAR && k >= 2) {
+            Ad = cmul(Ad, dz);
+            double2 c = s_coef[k - 1];
+            Ad = cadd(Ad, mk(c.x * (k - 1), c.y * (k - 1)));
+          }
+          A = cmul(A, dz);
+          double2 c = s_coef[k - 1];
+          A = cadd(A, mk(c.x, c.y));
+        }
+        A = cscale(A, sp.theta2);
+        A = cdivr(A, lhl);
+        cplx<double> a_local = cconj(A);
+        cplx<double> z = mk(x, y);
+        cplx<double> a_sm = alpha_smooth_(z, sp.kstar, sp.rect, corner, sp.approx, sp.taylor_smooth, sp.inv_pi);
+        cplx<double> w = cadd(cscale(z, 1.0 - sp.kappa), cscale(cconj(z), sp.gamma));
+        w = csub(csub(csub(w, a_star), a_local), a_sm);
+        if (VERT) {
+          w.re -= sp.cy_re;
+          w.im -= sp.cy_im;
+          double px = (w.re + sp.hly_re) * sp.npx / (2.0 * sp.hly_re);
+          double py = (w.im + sp.hly_im) * sp.npy / (2.0 * sp.hly_im);
+          verts[(size_t)j * (sp.nx) + i] = make_double2(px, double(sp.npy) - py);
+        } else {
+          if (isnan(w.re) || isnan(w.im)) continue;
+          w.re -= sp.cy_re;
+          w.im -= sp.cy_im;
+          if (w.re < -sp.hly_re || w.re > sp.hly_re || w.im < -sp.hly_im || w.im > sp.hly_im) continue;
+          double px = (w.re + sp.hly_re) * sp.npx / (2.0 * sp.hly_re);
+          double py = (w.im + sp.hly_im) * sp.npy / (2.0 * sp.hly_im);
+          bool pmin_ = false;
+          if (PAR) {
+            // mu = 1 / ((dw/dz)^2 - |dw/dzbar|^2)   (irs_functions.cuh:66-81)
+            cplx<double> dstar = mk(-(dr * sp.theta2), (di * sp.theta2));  // -theta^2 conj(sum m/d^2)
+            Ad = cscale(Ad, sp.theta2);
+            Ad = cdivr(Ad, lhl * lhl);
+            cplx<double> dloc = cconj(Ad);
+            double dsz = d_alpha_smooth_dz_(z, sp.kstar, sp.rect, corner, sp.approx);
+            cplx<double> dszb =
+                d_alpha_smooth_dzbar_(z, sp.kstar, sp.rect, corner, sp.approx, sp.taylor_smooth, sp.inv_pi);
+            double dwdz = (1.0 - sp.kappa) - dsz;
+            cplx<double> dwdzb = csub(csub(csub(mk(sp.gamma, 0.0), dstar), dloc), dszb);
+            double a = cabs_(dwdzb);
+            double mu = 1.0 / (dwdz * dwdz - a * a);
+            pmin_ = mu >= 0;
+          }
+          irs_deposit(px, py, sp.npx, sp.npy, pix, pmin, psad, pmin_, PAR);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ----------------------------------------------------------------- FP32 form
+// GENERIC_SMOOTH: the smooth sheet is not the circular approximation
+// (alpha_smooth = -kappa_star z); its deviation from that linear form is then
+// added per point in FP64.
+template <bool VERT, bool PAR, bool GENERIC_SMOOTH>
+__global__ void __launch_bounds__(kShootThreads) shoot_f32(ShootParams sp, LeafPtrs lp, long long total_tiles,
+                                                           int* __restrict__ pix, int* __restrict__ pmin,
+                                                           int* __restrict__ psad, double2* __restrict__ verts) {
+  constexpr int R = kRaysPerThread;
+  constexpr int RS = kShootThreads / kTileX;  // row stride between a thread's points
+  __shared__ float4 s_near[kMaxStarsDirect];
+  __shared__ float2 s_coef[kMaxOrder];
+  const int tx = threadIdx.x & (kTileX - 1), ty = threadIdx.x / kTileX;
+  const cplx<double> corner = mk(sp.corner_re, sp.corner_im);
+  // linear part of the lens equation for the circular approximation
+  const double lin_x = 1.0 - sp.kappa + sp.kstar + sp.gamma;
+  const double lin_y = 1.0 - sp.kappa + sp.kstar - sp.gamma;
+  const float flin_x = float(lin_x), flin_y = float(lin_y);
+  const double scx = sp.npx / (2.0 * sp.hly_re), scy = sp.npy / (2.0 * sp.hly_im);
+  const float step_y = float(2.0 * sp.rhs_y * RS);
+  for (long long t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+    TileInfo ti = tile_info(lp, t);
+    const int nn = lp.nnear[ti.leaf];
+    if (threadIdx.x < kMaxStarsDirect) {
+      float4 v = lp.near32[(size_t)ti.leaf * kMaxStarsDirect + threadIdx.x];
+      if (threadIdx.x >= nn) v = make_float4(1e18f, 1e18f, 0.f, 0.f);  // far away, zero mass
+      s_near[threadIdx.x] = v;
+    }
+    if (threadIdx.x >= 64 && threadIdx.x < 64 + kMaxOrder)
+      s_coef[threadIdx.x - 64] = lp.coef32[(size_t)ti.leaf * kMaxOrder + threadIdx.x - 64];
+    const double lcx = lp.cx[ti.leaf], lcy = lp.cy[ti.leaf];
+    const float inv_hl = float(1.0 / lp.hl[ti.leaf]);
+    // leaf-centre part of the source position, in pixel units
+    const double pcx = ((lin_x * lcx - sp.cy_re) + sp.hly_re) * scx;
+    const double pcy = ((lin_y * lcy - sp.cy_im) + sp.hly_im) * scy;
+    __syncthreads();
+    const int nn4 = (nn + 3) & ~3;
+    if (tx < ti.ni) {
+      const long long i = ti.i0 + tx;
+      const double xg = sp.base_x + 2.0 * (sp.rhs_x * double(i));
+      const float ux = float(xg - lcx);
+      const long long j0 = ti.j0 + ty;
+      const double yg0 = sp.base_y + 2.0 * (sp.rhs_y * double(j0));
+      const float uy0 = float(yg0 - lcy);
+      float uy[R];
+#pragma unroll
+      for (int r = 0; r < R; r++) uy[r] = uy0 + step_y * float(r);
+      // ---- near field, blocked compensated summation
+      float sx[R], sy[R], cxr[R], cyr[R];
+      float dxx[R], dxy[R];  // derivative sums (parity only)
+#pragma unroll
+      for (int r = 0; r < R; r++) sx[r] = sy[r] = cxr[r] = cyr[r] = dxx[r] = dxy[r] = 0.f;
+      for (int s0 = 0; s0 < nn4; s0 += 4) {
+        float bx[R], by[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) bx[r] = by[r] = 0.f;
+#pragma unroll
+        for (int s = 0; s < 4; s++) {
+          float4 st = s_near[s0 + s];
+#pragma unroll
+          for (int r = 0; r < R; r++) {
+            float ex = ux - st.x, ey = uy[r] - st.y;
+            float r2 = fmaf(ex, ex, ey * ey);
+            float inv = rcp_approx(r2);
+            float q = st.z * inv;
+            bx[r] = fmaf(q, ex, bx[r]);
+            by[r] = fmaf(q, ey, by[r]);
+            if (PAR) {
+              float t2 = q * inv;
+              dxx[r] = fmaf(t2, (ex - ey) * (ex + ey), dxx[r]);
+              dxy[r] = fmaf(t2, 2.f * ex * ey, dxy[r]);
+            }
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < R; r++) {  // two-sum of the block into the running sum
+          float s = sx[r] + bx[r];
+          float bb = s - sx[r];
+          cxr[r] += (sx[r] - (s - bb)) + (bx[r] - bb);
+          sx[r] = s;
+          s = sy[r] + by[r];
+          bb = s - sy[r];
+          cyr[r] += (sy[r] - (s - bb)) + (by[r] - bb);
+          sy[r] = s;
+        }
+      }
+      // ---- far field + output
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        const int jj = ty + r * RS;
+        if (jj >= ti.nj) break;
+        const long long j = ti.j0 + jj;
+        const float dzr = ux * inv_hl, dzi = uy[r] * inv_hl;
+        float Ar = 0.f, Ai = 0.f, Dr = 0.f, Di = 0.f;
+        for (int k = sp.p - 1; k >= 0; k--) {
+          if (PAR && k >= 1) {  // derivative polynomial sum k e_k dz^(k-1)
+            float tr = fmaf(Dr, dzr, -Di * dzi);
+            float tt = fmaf(Dr, dzi, Di * dzr);
+            float2 c = s_coef[k];
+            Dr = fmaf(c.x, float(k), tr);
+            Di = fmaf(c.y, float(k), tt);
+          }
+          float tr = fmaf(Ar, dzr, -Ai * dzi);
+          float tt = fmaf(Ar, dzi, Ai * dzr);
+          float2 c = s_coef[k];
+          Ar = tr + c.x;
+          Ai = tt + c.y;
+        }
+        const float Sx = sx[r] + cxr[r], Sy = sy[r] + cyr[r];
+        // w - w(centre) = lin * u - alpha_star - conj(A)
+        const float wr = fmaf(flin_x, ux, -(Sx + Ar));
+        const float wi = fmaf(flin_y, uy[r], -(Sy - Ai));
+        double px = pcx + double(wr) * scx;
+        double py = pcy + double(wi) * scy;
+        if (GENERIC_SMOOTH) {
+          cplx<double> z = mk(lcx + double(ux), lcy + double(uy[r]));
+          cplx<double> a_sm = alpha_smooth_(z, sp.kstar, sp.rect, corner, sp.approx, sp.taylor_smooth, sp.inv_pi);
+          px += (-a_sm.re - sp.kstar * z.re) * scx;
+          py += (-a_sm.im - sp.kstar * z.im) * scy;
+        }
+        if (VERT) {
+          verts[(size_t)j * (sp.nx) + i] = make_double2(px, double(sp.npy) - py);
+        } else {
+          if (!(px >= 0.0 && px <= double(sp.npx) && py >= 0.0 && py <= double(sp.npy))) continue;
+          bool pmin_ = false;
+          if (PAR) {
+            cplx<double> z = mk(lcx + double(ux), lcy + double(uy[r]));
+            double dsz = d_alpha_smooth_dz_(z, sp.kstar, sp.rect, corner, sp.approx);
+            cplx<double> dszb =
+                GENERIC_SMOOTH
+                    ? d_alpha_smooth_dzbar_(z, sp.kstar, sp.rect, corner, sp.approx, sp.taylor_smooth, sp.inv_pi)
+                    : mk(0.0, 0.0);
+            // d alpha_star / d zbar = -conj(sum m theta^2 / d^2) ; sum m/d^2 = sum q conj(d)^2/|d|^2
+            double dsr = -double(dxx[r]), dsi = -double(dxy[r]);
+            // d alpha_local / d zbar = conj(A'(dz)) / hl
+            double dlr = double(Dr) * double(inv_hl), dli = -double(Di) * double(inv_hl);
+            double dwdz = (1.0 - sp.kappa) - dsz;
+            double gr = sp.gamma - dsr - dlr - dszb.re, gi = -dsi - dli - dszb.im;
+            double mu = 1.0 / (dwdz * dwdz - (gr * gr + gi * gi));
+            pmin_ = mu >= 0;
+          }
+          irs_deposit(px, py, sp.npx, sp.npy, pix, pmin, psad, pmin_, PAR);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace irsb

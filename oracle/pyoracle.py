@@ -1,0 +1,180 @@
+"""ctypes wrapper of oracle/liboracle.so -- test infrastructure only.
+
+The CPU oracle restates the reference algorithm in FP64 (see oracle.c). Only
+tests, the smoke check and the benchmark's CPU-baseline leg use it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+
+class OrcLens(C.Structure):
+    _fields_ = [("kappa", C.c_double), ("gamma", C.c_double), ("kstar", C.c_double), ("theta", C.c_double),
+                ("rect", C.c_int), ("approx", C.c_int), ("taylor_smooth", C.c_int),
+                ("corner_re", C.c_double), ("corner_im", C.c_double)]
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        vp, d, i, ll = C.c_void_p, C.c_double, C.c_int, C.c_longlong
+        L.orc_tree_build.argtypes = [i, vp, d, i, d, d]
+        L.orc_tree_build.restype = vp
+        L.orc_tree_free.argtypes = [vp]
+        for f in ["orc_tree_num_nodes", "orc_tree_levels", "orc_tree_order", "orc_tree_overflow"]:
+            getattr(L, f).argtypes = [vp]
+            getattr(L, f).restype = i
+        L.orc_tree_stars.argtypes = [vp, vp]
+        L.orc_tree_nodes.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.orc_tree_coeffs.argtypes = [vp, vp, vp]
+        L.orc_shoot_fmm.argtypes = [vp, C.POINTER(OrcLens), ll, vp, vp, vp, vp, vp]
+        L.orc_shoot_direct.argtypes = [i, vp, C.POINTER(OrcLens), ll, vp, vp, vp, vp, i]
+        L.orc_shoot_direct_lattice.argtypes = [i, vp, C.POINTER(OrcLens), d, d, d, d, ll, ll, ll, ll, vp, vp, i]
+        L.orc_irs_bin.argtypes = [ll, vp, vp, vp, d, d, d, d, i, i, vp, vp, vp]
+        L.orc_ipm_deposit_ref.argtypes = [ll, ll, vp, vp, d, i, i, vp, vp, vp, i]
+        L.orc_ipm_deposit_fix_f32.argtypes = [ll, ll, vp, C.c_float, i, i, vp, vp, vp, i]
+        L.orc_ipm_deposit_fix_f64.argtypes = [ll, ll, vp, d, i, i, vp, vp, vp, i]
+        L.orc_derive.argtypes = [d, d, d, d, d, d, d, i, d, d, d, d, d, i, i, i, vp]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data
+
+
+def lens(kappa, gamma, kstar, theta, rect=0, approx=1, taylor_smooth=1, corner=(0.0, 0.0)):
+    return OrcLens(float(kappa), float(gamma), float(kstar), float(theta), int(rect), int(approx),
+                   int(taylor_smooth), float(corner[0]), float(corner[1]))
+
+
+class Tree:
+    """Quadtree + expansions of the reference algorithm (FP64)."""
+
+    def __init__(self, stars, root_hl, order=0, theta=1.0, alpha_error=1e-3):
+        s = np.ascontiguousarray(np.asarray(stars, np.float64).reshape(-1, 3))
+        self.h = lib().orc_tree_build(int(s.shape[0]), _p(s), float(root_hl), int(order), float(theta),
+                                      float(alpha_error))
+        self.n = lib().orc_tree_num_nodes(self.h)
+        self.levels = lib().orc_tree_levels(self.h)
+        self.order = lib().orc_tree_order(self.h)
+        self.overflow = lib().orc_tree_overflow(self.h)
+        self.nstars = s.shape[0]
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_tree_free(self.h)
+            self.h = None
+
+    def stars(self):
+        out = np.zeros((self.nstars, 3))
+        lib().orc_tree_stars(self.h, _p(out))
+        return out
+
+    def arrays(self):
+        ints = np.zeros((self.n, 8), np.int32)
+        geom = np.zeros((self.n, 3))
+        nbr = np.zeros((self.n, 8), np.int32)
+        sil = np.zeros((self.n, 27), np.int32)
+        dil = np.zeros((self.n, 5), np.int32)
+        lib().orc_tree_nodes(self.h, _p(ints), _p(geom), _p(nbr), _p(sil), _p(dil))
+        return ints, geom, nbr, sil, dil
+
+    def coeffs(self):
+        m = np.zeros((self.n, self.order + 1, 2))
+        l = np.zeros((self.n, self.order + 1, 2))
+        lib().orc_tree_coeffs(self.h, _p(m), _p(l))
+        return m[..., 0] + 1j * m[..., 1], l[..., 0] + 1j * l[..., 1]
+
+    def shoot(self, lens_, zx, zy, want_mu=False):
+        zx = np.ascontiguousarray(zx, np.float64).ravel()
+        zy = np.ascontiguousarray(zy, np.float64).ravel()
+        wx = np.zeros_like(zx)
+        wy = np.zeros_like(zy)
+        mu = np.zeros_like(zx) if want_mu else None
+        lib().orc_shoot_fmm(self.h, C.byref(lens_), zx.size, _p(zx), _p(zy), _p(wx), _p(wy),
+                            _p(mu) if want_mu else None)
+        return (wx, wy, mu) if want_mu else (wx, wy)
+
+
+def shoot_direct(stars, lens_, zx, zy, threads=0):
+    s = np.ascontiguousarray(np.asarray(stars, np.float64).reshape(-1, 3))
+    zx = np.ascontiguousarray(zx, np.float64).ravel()
+    zy = np.ascontiguousarray(zy, np.float64).ravel()
+    wx = np.zeros_like(zx)
+    wy = np.zeros_like(zy)
+    lib().orc_shoot_direct(s.shape[0], _p(s), C.byref(lens_), zx.size, _p(zx), _p(zy), _p(wx), _p(wy), threads)
+    return wx, wy
+
+
+def shoot_direct_lattice(stars, lens_, bx, by, rx, ry, i0, ni, j0, nj, threads=0):
+    s = np.ascontiguousarray(np.asarray(stars, np.float64).reshape(-1, 3))
+    wx = np.zeros((nj, ni))
+    wy = np.zeros((nj, ni))
+    lib().orc_shoot_direct_lattice(s.shape[0], _p(s), C.byref(lens_), bx, by, rx, ry, i0, ni, j0, nj, _p(wx),
+                                   _p(wy), threads)
+    return wx, wy
+
+
+def irs_bin(wx, wy, center, hly, npix, mu=None):
+    wx = np.ascontiguousarray(wx, np.float64).ravel()
+    wy = np.ascontiguousarray(wy, np.float64).ravel()
+    pix = np.zeros((npix[1], npix[0]), np.int32)
+    pmin = np.zeros_like(pix)
+    psad = np.zeros_like(pix)
+    m = None if mu is None else np.ascontiguousarray(mu, np.float64).ravel()
+    lib().orc_irs_bin(wx.size, _p(wx), _p(wy), _p(m) if m is not None else None, center[0], center[1], hly[0],
+                      hly[1], npix[0], npix[1], _p(pix), _p(pmin), _p(psad))
+    return (pix, pmin, psad) if mu is not None else pix
+
+
+def ipm_deposit_ref(verts, factor, npix, parities=False):
+    """verts: (ny+1, nx+1, 2) vertex pixel positions (row axis flipped)."""
+    v = np.ascontiguousarray(verts, np.float64)
+    ncy, ncx = v.shape[0] - 1, v.shape[1] - 1
+    vx = np.ascontiguousarray(v[..., 0])
+    vy = np.ascontiguousarray(v[..., 1])
+    pix = np.zeros((npix[1], npix[0]))
+    pmin = np.zeros_like(pix)
+    psad = np.zeros_like(pix)
+    lib().orc_ipm_deposit_ref(ncx, ncy, _p(vx), _p(vy), float(factor), npix[0], npix[1], _p(pix), _p(pmin),
+                              _p(psad), int(parities))
+    return (pix, pmin, psad) if parities else pix
+
+
+def ipm_deposit_fixed(verts, factor, npix, parities=False, single=True):
+    v = np.ascontiguousarray(verts, np.float64)
+    ncy, ncx = v.shape[0] - 1, v.shape[1] - 1
+    mt = np.zeros((npix[1], npix[0]), np.uint64)
+    mn = np.zeros_like(mt)
+    ms = np.zeros_like(mt)
+    f = lib().orc_ipm_deposit_fix_f32 if single else lib().orc_ipm_deposit_fix_f64
+    f(ncx, ncy, _p(v), factor, npix[0], npix[1], _p(mt), _p(mn), _p(ms), int(parities))
+    return (mn, ms) if parities else mt
+
+
+def derive(kappa, gamma, kstar, theta, mean_mass, mean_mass2, light_loss, rect, safety, center, hly, npix, nry):
+    out = np.zeros(14)
+    lib().orc_derive(kappa, gamma, kstar, theta, mean_mass, mean_mass2, light_loss, int(rect), safety, center[0],
+                     center[1], hly[0], hly[1], npix[0], npix[1], nry, _p(out))
+    keys = ["mu_ave", "num_rays_x", "ray_half_sep_1", "ray_half_sep_2", "half_length_x1", "half_length_x2",
+            "num_ray_threads_1", "num_ray_threads_2", "center_x1", "center_x2", "num_stars", "corner_x1",
+            "corner_x2", "alpha_error"]
+    return dict(zip(keys, out))

@@ -1,0 +1,83 @@
+"""End-to-end behaviour of the Python / C-ABI interface on the GPU."""
+import os
+
+import numpy as np
+import pytest
+
+import irs_b200
+from tests.cases import IPM_SMALL, IRS_SMALL
+
+pytestmark = pytest.mark.gpu
+
+
+def test_ipm_run_and_save_files(gpu, tmp_path):
+    m = irs_b200.IPM(**{**IPM_SMALL, "write_histograms": 1}, outfile_prefix=str(tmp_path) + "/",
+                     write_parities=True)
+    m.run()
+    assert m.magnifications.shape == (m.num_pixels_y2, m.num_pixels_y1)
+    assert m.stars.shape == (m.num_stars, 3)
+    assert m.t_shoot_cells > 0
+    m.save()
+    for f in ["ipm_parameter_info.txt", "ipm_stars.bin", "ipm_magnifications.bin", "ipm_magnifications_minima.bin",
+              "ipm_magnifications_saddles.bin", "ipm_mags_numpixels.txt", "ipm_log_mags_numpixels.txt"]:
+        assert os.path.exists(tmp_path / f), f
+    raw = np.fromfile(tmp_path / "ipm_magnifications.bin", dtype=np.int32, count=2)
+    assert list(raw) == [m.num_pixels_y2, m.num_pixels_y1]
+    arr = np.fromfile(tmp_path / "ipm_magnifications.bin", dtype=np.float32, offset=8)
+    np.testing.assert_array_equal(arr.reshape(m.magnifications.shape), m.magnifications)
+    hist = np.loadtxt(tmp_path / "ipm_mags_numpixels.txt", dtype=np.int64)
+    assert hist[:, 1].sum() == m.magnifications.size
+    info = dict(l.split() for l in open(tmp_path / "ipm_parameter_info.txt"))
+    assert int(info["num_stars"]) == m.num_stars
+
+
+def test_star_generation_statistics(gpu):
+    m = irs_b200.IPM(**IPM_SMALL, is_double=True)
+    m.run()
+    s = m.stars
+    r = np.hypot(s[:, 0], s[:, 1])
+    R = m.corner[0]
+    assert r.max() <= R * (1 + 1e-12)
+    # uniform in the disc: P(r < R/sqrt(2)) = 1/2
+    frac = np.mean(r < R / np.sqrt(2))
+    assert abs(frac - 0.5) < 4 / np.sqrt(len(r))
+    assert s[:, 2].min() >= 0.08 - 1e-12 and s[:, 2].max() <= 1.0 + 1e-12
+    assert abs(s[:, 2].mean() - m.value("mean_mass")) < 5 * s[:, 2].std() / np.sqrt(len(s))
+
+
+def test_same_seed_same_stars_float_double(gpu):
+    a = irs_b200.IRS(**IRS_SMALL, is_double=True)
+    b = irs_b200.IRS(**IRS_SMALL, is_double=False)
+    a.run()
+    b.run()
+    if a.num_stars != b.num_stars:
+        pytest.skip("float and double derivations round num_stars differently for this case")
+    sa = a.stars[np.lexsort(a.stars.T[::-1])]
+    sb = b.stars.astype(np.float64)[np.lexsort(b.stars.T[::-1].astype(np.float64))]
+    assert sa.shape == sb.shape
+    assert np.abs(sa - sb).max() < 1e-4
+
+
+def test_host_star_field(gpu):
+    a = irs_b200.IRS(**IRS_SMALL, is_double=True)
+    a.run()
+    b = irs_b200.IRS(**IRS_SMALL, is_double=True, safety_scale=1.3)
+    b.set_stars(a.stars, rectangular=False, corner=a.corner, theta_star=a.theta_star)
+    b.run()
+    assert b.num_stars == a.num_stars
+    assert np.abs(a.magnifications.astype(np.int64) - b.magnifications).sum() <= 2
+
+
+def test_run_failure_raises(gpu):
+    m = irs_b200.IPM(kappa_tot=0.45, shear=0.55, kappa_star=0.2)
+    with pytest.raises(Exception, match="Error running IPM"):
+        m.run()
+
+
+def test_expansion_order_default_is_reference_formula(gpu):
+    m = irs_b200.IRS(**IRS_SMALL, is_double=True)
+    m.run()
+    import math
+    p = math.ceil(2 * math.log2(m.theta_star) + m.value("tree_levels") - math.log2(m.value("root_half_length"))
+                  - math.log2(m.value("alpha_error")))
+    assert m.expansion_order == p
