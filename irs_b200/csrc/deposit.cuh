@@ -170,12 +170,26 @@ __device__ __forceinline__ D dabs(D a) {
   return a < D(0) ? -a : a;
 }
 
+// Output of the deposition: per-pixel fixed-point pieces plus a per-row
+// difference array for runs of fully covered pixels (row stride npx + 1).
+struct DepositMaps {
+  unsigned long long* acc;   // [npy][npx] boundary pieces
+  unsigned long long* diff;  // [npy][npx + 1] span starts (+q) and ends (-q), modulo 2^64
+};
+
 // Deposits triangle (a, b, c) given in absolute pixel coordinates (row axis
 // already flipped). factor = image-plane area of the triangle in pixel units.
+//
+// Sweep: the triangle is clipped to the map, then cut into row strips
+// [y, y+1] (bottom to top). Within a strip, the columns between the left and
+// right boundaries that lie inside both the strip's bottom edge (on y) and
+// its top edge (on y+1) are fully covered: by convexity the unit pixel is
+// inside, so its clipped area is exactly 1 and the run [xa, xb) is recorded
+// as one +q / -q pair in the difference array. The remaining boundary columns
+// are clipped one at a time (left to right) and their areas added as pieces.
 template <typename D>
 __device__ void deposit_triangle(double ax, double ay, double bx, double by, double cx, double cy, D factor,
-                                 int npx, int npy, unsigned long long* __restrict__ map_total,
-                                 unsigned long long* __restrict__ map_min, unsigned long long* __restrict__ map_sad,
+                                 int npx, int npy, DepositMaps m_total, DepositMaps m_min, DepositMaps m_sad,
                                  bool parities) {
   if (isnan(ax) || isnan(ay) || isnan(bx) || isnan(by) || isnan(cx) || isnan(cy)) return;
   double fx = floor(fmin(ax, fmin(bx, cx)));
@@ -192,13 +206,14 @@ __device__ void deposit_triangle(double ax, double ay, double bx, double by, dou
   P.y[2] = D(cy - fy);
   D A = P.area();
   if (!(dabs(A) < RN<D>::mul(D(10000), factor))) return;
-  unsigned long long* map = parities ? (A < D(0) ? map_min : map_sad) : map_total;
+  DepositMaps M = parities ? (A < D(0) ? m_min : m_sad) : m_total;
   // map edges in local coordinates (exact: integers)
   const D X0 = D(-ox), X1 = D(npx - ox), Y0 = D(-oy), Y1 = D(npy - oy);
   if (P.min_x() >= X1 || P.max_x() <= X0 || P.min_y() >= Y1 || P.max_y() <= Y0) return;
   D whole = dabs(A);
   if (whole == D(0)) return;
   const D scale = RN<D>::div(RN<D>::mul(factor, D(kFixScale)), whole);
+  const unsigned long long qfull = RN<D>::to_fix(scale);
   Poly<D> lo, hi;
   if (P.min_x() < X0) {
     clip_x(P, X0, lo, hi);
@@ -217,37 +232,63 @@ __device__ void deposit_triangle(double ax, double ay, double bx, double by, dou
     P = lo;
   }
   if (P.n < 3) return;
-  int xmin = int(P.min_x()), xmax = int(P.max_x());
-  if (xmax + ox == npx) xmax--;
-  for (int x = xmin; x < xmax; x++) {
-    Poly<D> L;
-    clip_x(P, D(x + 1), L, hi);
-    P = hi;
-    if (L.n < 3) continue;
-    int ymin = int(L.min_y()), ymax = int(L.max_y());
-    if (ymax + oy == npy) ymax--;
-    const long long col = ox + x;
-    for (int y = ymin; y < ymax; y++) {
-      Poly<D> B, Tp;
-      clip_y(L, D(y + 1), B, Tp);
-      L = Tp;
-      if (B.n < 3) continue;
-      fix_add<D>(map, (oy + y) * (long long)npx + col, dabs(B.area()), scale);
-    }
-    fix_add<D>(map, (oy + ymax) * (long long)npx + col, dabs(L.area()), scale);
-  }
-  if (P.n < 3) return;
   int ymin = int(P.min_y()), ymax = int(P.max_y());
   if (ymax + oy == npy) ymax--;
-  const long long col = ox + xmax;
-  for (int y = ymin; y < ymax; y++) {
-    Poly<D> B, Tp;
-    clip_y(P, D(y + 1), B, Tp);
-    P = Tp;
-    if (B.n < 3) continue;
-    fix_add<D>(map, (oy + y) * (long long)npx + col, dabs(B.area()), scale);
+  const long long rstride = (long long)npx + 1;
+  for (int y = ymin; y <= ymax; y++) {
+    Poly<D> S;
+    if (y < ymax) {
+      clip_y(P, D(y + 1), S, hi);
+      P = hi;
+    } else {
+      S = P;
+    }
+    if (S.n < 3) continue;
+    const long long row = oy + y;
+    // full-coverage run from the strip's bottom (y) and top (y + 1) edges
+    const D yb = D(y), yt = D(y + 1);
+    D b0 = D(0), b1 = D(0), t0 = D(0), t1 = D(0);
+    bool hb = false, ht = false;
+    for (int i = 0; i < S.n; i++) {
+      D vx = S.x[i], vy = S.y[i];
+      if (vy == yb) {
+        b0 = hb ? (vx < b0 ? vx : b0) : vx;
+        b1 = hb ? (vx > b1 ? vx : b1) : vx;
+        hb = true;
+      }
+      if (vy == yt) {
+        t0 = ht ? (vx < t0 ? vx : t0) : vx;
+        t1 = ht ? (vx > t1 ? vx : t1) : vx;
+        ht = true;
+      }
+    }
+    int xa = 1, xb = 0;
+    if (hb && ht) {
+      D l = b0 > t0 ? b0 : t0, r = b1 < t1 ? b1 : t1;
+      xa = int(ceil(l));
+      xb = int(floor(r));
+    }
+    int xmin = int(S.min_x()), xmax = int(S.max_x());
+    if (xmax + ox == npx) xmax--;
+    Poly<D> R = S;
+    int x = xmin;
+    while (x < xmax) {
+      if (xa < xb && x == xa) {
+        clip_x(R, D(xb), lo, hi);
+        R = hi;
+        atomicAdd(M.diff + row * rstride + (ox + xa), qfull);
+        atomicAdd(M.diff + row * rstride + (ox + xb), (unsigned long long)(0ULL - qfull));
+        x = xb;
+        continue;
+      }
+      Poly<D> L;
+      clip_x(R, D(x + 1), L, hi);
+      R = hi;
+      if (L.n >= 3) fix_add<D>(M.acc, row * npx + (ox + x), dabs(L.area()), scale);
+      x++;
+    }
+    if (x == xmax) fix_add<D>(M.acc, row * npx + (ox + xmax), dabs(R.area()), scale);
   }
-  fix_add<D>(map, (oy + ymax) * (long long)npx + col, dabs(P.area()), scale);
 }
 
 // One thread per lens-plane cell (i, j) of an ncx x ncy cell lattice whose
@@ -255,9 +296,8 @@ __device__ void deposit_triangle(double ax, double ay, double bx, double by, dou
 template <typename D>
 __global__ void __launch_bounds__(256) ipm_deposit_cells(const double2* __restrict__ verts, long long ncx,
                                                          long long ncy, D factor, int npx, int npy,
-                                                         unsigned long long* __restrict__ map_total,
-                                                         unsigned long long* __restrict__ map_min,
-                                                         unsigned long long* __restrict__ map_sad, int parities) {
+                                                         DepositMaps m_total, DepositMaps m_min, DepositMaps m_sad,
+                                                         int parities) {
   const long long ncells = ncx * ncy;
   const long long vx = ncx + 1;
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncells;
@@ -267,10 +307,32 @@ __global__ void __launch_bounds__(256) ipm_deposit_cells(const double2* __restri
     double2 y1 = verts[(j + 1) * vx + i];        // z - conj(rhs)
     double2 y2 = verts[j * vx + i];              // z - rhs
     double2 y3 = verts[j * vx + (i + 1)];        // z + conj(rhs)
-    deposit_triangle<D>(y0.x, y0.y, y1.x, y1.y, y2.x, y2.y, factor, npx, npy, map_total, map_min, map_sad,
+    deposit_triangle<D>(y0.x, y0.y, y1.x, y1.y, y2.x, y2.y, factor, npx, npy, m_total, m_min, m_sad,
                         parities != 0);
-    deposit_triangle<D>(y2.x, y2.y, y3.x, y3.y, y0.x, y0.y, factor, npx, npy, map_total, map_min, map_sad,
+    deposit_triangle<D>(y2.x, y2.y, y3.x, y3.y, y0.x, y0.y, factor, npx, npy, m_total, m_min, m_sad,
                         parities != 0);
+  }
+}
+
+// Row prefix sum of the difference array added to the pieces: one warp per
+// row, 32 columns per step with a carried running sum (integer, exact).
+__global__ void ipm_resolve_rows(int npx, int npy, DepositMaps m) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int y = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; y < npy; y += warps) {
+    unsigned long long carry = 0;
+    const long long rs = (long long)npx + 1;
+    for (int x0 = 0; x0 < npx; x0 += 32) {
+      int x = x0 + lane;
+      unsigned long long v = x < npx ? m.diff[y * rs + x] : 0ULL;
+      for (int o = 1; o < 32; o <<= 1) {
+        unsigned long long u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+      }
+      v += carry;
+      if (x < npx) m.acc[(long long)y * npx + x] += v;
+      carry = __shfl_sync(0xffffffffu, v, 31);
+    }
   }
 }
 

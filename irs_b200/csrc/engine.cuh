@@ -382,6 +382,7 @@ class MapMaker {
   LatticeTiles tiles_;
   DevVec<int> d_pix_, d_pmin_, d_psad_;
   DevVec<unsigned long long> d_acc_, d_acc_min_, d_acc_sad_;
+  DevVec<unsigned long long> d_diff_, d_diff_min_, d_diff_sad_;
   DevVec<T> d_map_, d_map_min_, d_map_sad_;
   DevVec<double2> d_verts_;
   DevVec<unsigned long long> d_red_;
@@ -520,16 +521,21 @@ class MapMaker {
     } else {
       const long long nverts = sp.nx * sp.ny;
       if (!d_verts_.alloc_exact(nverts)) return false;
-      if (!d_acc_.alloc_exact(npix) || !d_map_.alloc_exact(npix)) return false;
+      const long long ndiff = (long long)p.num_pixels_y.im * (p.num_pixels_y.re + 1);
+      if (!d_acc_.alloc_exact(npix) || !d_map_.alloc_exact(npix) || !d_diff_.alloc_exact(ndiff)) return false;
       if (par && (!d_acc_min_.alloc_exact(npix) || !d_acc_sad_.alloc_exact(npix) || !d_map_min_.alloc_exact(npix) ||
-                  !d_map_sad_.alloc_exact(npix)))
+                  !d_map_sad_.alloc_exact(npix) || !d_diff_min_.alloc_exact(ndiff) || !d_diff_sad_.alloc_exact(ndiff)))
         return false;
       IRSB_CKR(cudaEventRecord(ev1_, stream_));
       IRSB_CKR(cudaMemsetAsync(d_acc_.p, 0, npix * sizeof(unsigned long long), stream_));
+      IRSB_CKR(cudaMemsetAsync(d_diff_.p, 0, ndiff * sizeof(unsigned long long), stream_));
       if (par) {
         IRSB_CKR(cudaMemsetAsync(d_acc_min_.p, 0, npix * sizeof(unsigned long long), stream_));
         IRSB_CKR(cudaMemsetAsync(d_acc_sad_.p, 0, npix * sizeof(unsigned long long), stream_));
+        IRSB_CKR(cudaMemsetAsync(d_diff_min_.p, 0, ndiff * sizeof(unsigned long long), stream_));
+        IRSB_CKR(cudaMemsetAsync(d_diff_sad_.p, 0, ndiff * sizeof(unsigned long long), stream_));
       }
+      DepositMaps mt{d_acc_.p, d_diff_.p}, mmin{d_acc_min_.p, d_diff_min_.p}, msad{d_acc_sad_.p, d_diff_sad_.p};
       if (!launch_shoot<true>(sp, nullptr, nullptr, nullptr, d_verts_.p)) return false;
       const long long ncx = p.num_ray_threads.re, ncy = p.num_ray_threads.im;
       long long ncells = ncx * ncy;
@@ -538,18 +544,26 @@ class MapMaker {
         float factor = float(2 * p.ray_half_sep.re * p.ray_half_sep.im * p.num_pixels_y.re * p.num_pixels_y.im /
                              (2 * p.half_length_y.re * 2 * p.half_length_y.im));
         ipm_deposit_cells<float><<<grid, 256, 0, stream_>>>(d_verts_.p, ncx, ncy, factor, p.num_pixels_y.re,
-                                                            p.num_pixels_y.im, d_acc_.p, d_acc_min_.p, d_acc_sad_.p,
-                                                            par ? 1 : 0);
+                                                            p.num_pixels_y.im, mt, mmin, msad, par ? 1 : 0);
       } else {
         double factor = double(2 * p.ray_half_sep.re * p.ray_half_sep.im * p.num_pixels_y.re * p.num_pixels_y.im /
                                (2 * p.half_length_y.re * 2 * p.half_length_y.im));
         ipm_deposit_cells<double><<<grid, 256, 0, stream_>>>(d_verts_.p, ncx, ncy, factor, p.num_pixels_y.re,
-                                                             p.num_pixels_y.im, d_acc_.p, d_acc_min_.p, d_acc_sad_.p,
-                                                             par ? 1 : 0);
+                                                             p.num_pixels_y.im, mt, mmin, msad, par ? 1 : 0);
       }
       IRSB_LAUNCH_CK("ipm_deposit_cells");
       IRSB_CKR(cudaEventRecord(ev_dep1_, stream_));
-      launches += 2;
+      {
+        int gr = std::max(1, std::min(ceil_div((long long)p.num_pixels_y.im * 32, 256), 148 * 8));
+        if (par) {
+          ipm_resolve_rows<<<gr, 256, 0, stream_>>>(p.num_pixels_y.re, p.num_pixels_y.im, mmin);
+          ipm_resolve_rows<<<gr, 256, 0, stream_>>>(p.num_pixels_y.re, p.num_pixels_y.im, msad);
+        } else {
+          ipm_resolve_rows<<<gr, 256, 0, stream_>>>(p.num_pixels_y.re, p.num_pixels_y.im, mt);
+        }
+        IRSB_LAUNCH_CK("ipm_resolve_rows");
+      }
+      launches += par ? 4 : 3;
       int g2 = int(std::max<long long>(1, std::min<long long>((npix + 255) / 256, 148LL * 16)));
       ipm_finalize<T><<<g2, 256, 0, stream_>>>(npix, d_acc_.p, d_acc_min_.p, d_acc_sad_.p, d_map_.p, d_map_min_.p,
                                                  d_map_sad_.p, par ? 1 : 0);

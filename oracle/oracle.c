@@ -1126,37 +1126,61 @@ void orc_ipm_deposit_ref(long long ncx, long long ncy, const double* vx, const d
       P = lo;                                                                                              \
     }                                                                                                      \
     if (P.n < 3) return;                                                                                   \
-    int xmin = (int)fp_minx_##SUF(&P), xmax = (int)fp_maxx_##SUF(&P);                                      \
-    if (xmax + ox == npx) xmax--;                                                                          \
-    for (int x = xmin; x < xmax; x++) {                                                                    \
-      FP_##SUF L;                                                                                          \
-      fp_clipx_##SUF(&P, (D)(x + 1), &L, &hi);                                                             \
-      P = hi;                                                                                              \
-      if (L.n < 3) continue;                                                                               \
-      int ymin = (int)fp_miny_##SUF(&L), ymax = (int)fp_maxy_##SUF(&L);                                    \
-      if (ymax + oy == npy) ymax--;                                                                        \
-      long long col = ox + x;                                                                              \
-      for (int y = ymin; y < ymax; y++) {                                                                  \
-        FP_##SUF B, Tp;                                                                                    \
-        fp_clipy_##SUF(&L, (D)(y + 1), &B, &Tp);                                                           \
-        L = Tp;                                                                                            \
-        if (B.n < 3) continue;                                                                             \
-        fp_fix_##SUF(map, (oy + y) * (long long)npx + col, fp_abs_##SUF(fp_area_##SUF(&B)), scale);        \
-      }                                                                                                    \
-      fp_fix_##SUF(map, (oy + ymax) * (long long)npx + col, fp_abs_##SUF(fp_area_##SUF(&L)), scale);       \
-    }                                                                                                      \
-    if (P.n < 3) return;                                                                                   \
+    uint64_t qfull = (uint64_t)RINT(scale);                                                                \
     int ymin = (int)fp_miny_##SUF(&P), ymax = (int)fp_maxy_##SUF(&P);                                      \
     if (ymax + oy == npy) ymax--;                                                                          \
-    long long col = ox + xmax;                                                                             \
-    for (int y = ymin; y < ymax; y++) {                                                                    \
-      FP_##SUF B, Tp;                                                                                      \
-      fp_clipy_##SUF(&P, (D)(y + 1), &B, &Tp);                                                             \
-      P = Tp;                                                                                              \
-      if (B.n < 3) continue;                                                                               \
-      fp_fix_##SUF(map, (oy + y) * (long long)npx + col, fp_abs_##SUF(fp_area_##SUF(&B)), scale);          \
+    for (int y = ymin; y <= ymax; y++) {                                                                   \
+      FP_##SUF S;                                                                                          \
+      if (y < ymax) {                                                                                      \
+        fp_clipy_##SUF(&P, (D)(y + 1), &S, &hi);                                                           \
+        P = hi;                                                                                            \
+      } else {                                                                                             \
+        S = P;                                                                                             \
+      }                                                                                                    \
+      if (S.n < 3) continue;                                                                               \
+      long long row = oy + y;                                                                              \
+      D yb = (D)y, yt = (D)(y + 1);                                                                        \
+      D b0 = 0, b1 = 0, t0 = 0, t1 = 0;                                                                    \
+      int hb = 0, ht = 0;                                                                                  \
+      for (int i = 0; i < S.n; i++) {                                                                      \
+        D vx = S.x[i], vy = S.y[i];                                                                        \
+        if (vy == yb) {                                                                                    \
+          b0 = hb ? (vx < b0 ? vx : b0) : vx;                                                              \
+          b1 = hb ? (vx > b1 ? vx : b1) : vx;                                                              \
+          hb = 1;                                                                                          \
+        }                                                                                                  \
+        if (vy == yt) {                                                                                    \
+          t0 = ht ? (vx < t0 ? vx : t0) : vx;                                                              \
+          t1 = ht ? (vx > t1 ? vx : t1) : vx;                                                              \
+          ht = 1;                                                                                          \
+        }                                                                                                  \
+      }                                                                                                    \
+      int xa = 1, xb = 0;                                                                                  \
+      if (hb && ht) {                                                                                      \
+        D l = b0 > t0 ? b0 : t0, r = b1 < t1 ? b1 : t1;                                                    \
+        xa = (int)ceil((double)l);                                                                         \
+        xb = (int)floor((double)r);                                                                        \
+      }                                                                                                    \
+      int xmin = (int)fp_minx_##SUF(&S), xmax = (int)fp_maxx_##SUF(&S);                                    \
+      if (xmax + ox == npx) xmax--;                                                                        \
+      FP_##SUF R = S;                                                                                      \
+      int x = xmin;                                                                                        \
+      while (x < xmax) {                                                                                   \
+        if (xa < xb && x == xa) {                                                                          \
+          fp_clipx_##SUF(&R, (D)xb, &lo, &hi);                                                             \
+          R = hi;                                                                                          \
+          for (int c = xa; c < xb; c++) map[row * npx + ox + c] += qfull;                                  \
+          x = xb;                                                                                          \
+          continue;                                                                                        \
+        }                                                                                                  \
+        FP_##SUF Lp;                                                                                       \
+        fp_clipx_##SUF(&R, (D)(x + 1), &Lp, &hi);                                                          \
+        R = hi;                                                                                            \
+        if (Lp.n >= 3) fp_fix_##SUF(map, row * npx + ox + x, fp_abs_##SUF(fp_area_##SUF(&Lp)), scale);     \
+        x++;                                                                                               \
+      }                                                                                                    \
+      if (x == xmax) fp_fix_##SUF(map, row * npx + ox + xmax, fp_abs_##SUF(fp_area_##SUF(&R)), scale);     \
     }                                                                                                      \
-    fp_fix_##SUF(map, (oy + ymax) * (long long)npx + col, fp_abs_##SUF(fp_area_##SUF(&P)), scale);         \
   }                                                                                                        \
   void orc_ipm_deposit_fix_##SUF(long long ncx, long long ncy, const double* vxy, D factor, int npx, int npy, \
                                  uint64_t* mt, uint64_t* mmin, uint64_t* msad, int parities) {             \

@@ -148,6 +148,7 @@ def irs_bin(wx, wy, center, hly, npix, mu=None):
 def ipm_deposit_ref(verts, factor, npix, parities=False):
     """verts: (ny+1, nx+1, 2) vertex pixel positions (row axis flipped)."""
     v = np.ascontiguousarray(verts, np.float64)
+    assert v.ndim == 3 and v.shape[2] == 2, "verts must be (ny+1, nx+1, 2)"
     ncy, ncx = v.shape[0] - 1, v.shape[1] - 1
     vx = np.ascontiguousarray(v[..., 0])
     vy = np.ascontiguousarray(v[..., 1])
@@ -161,6 +162,7 @@ def ipm_deposit_ref(verts, factor, npix, parities=False):
 
 def ipm_deposit_fixed(verts, factor, npix, parities=False, single=True):
     v = np.ascontiguousarray(verts, np.float64)
+    assert v.ndim == 3 and v.shape[2] == 2, "verts must be (ny+1, nx+1, 2)"
     ncy, ncx = v.shape[0] - 1, v.shape[1] - 1
     mt = np.zeros((npix[1], npix[0]), np.uint64)
     mn = np.zeros_like(mt)
@@ -178,3 +180,112 @@ def derive(kappa, gamma, kstar, theta, mean_mass, mean_mass2, light_loss, rect, 
             "num_ray_threads_1", "num_ray_threads_2", "center_x1", "center_x2", "num_stars", "corner_x1",
             "corner_x2", "alpha_error"]
     return dict(zip(keys, out))
+
+
+# ---------------------------------------------------------------- reference code on the host
+REFDIR = os.path.join(HERE, "_ref")
+
+
+class RefLens(C.Structure):
+    _fields_ = OrcLens._fields_
+
+
+_ref = {}
+
+
+def ref_available() -> bool:
+    return all(os.path.exists(os.path.join(REFDIR, f)) for f in ("libref_ipm.so", "libref_irs.so"))
+
+
+def build_ref():
+    """Compile the reference's headers for the host (needs the reference sources)."""
+    subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+def ref_lib(kind="ipm"):
+    if kind not in _ref:
+        L = C.CDLL(os.path.join(REFDIR, f"libref_{kind}.so"))
+        vp, d, i, ll = C.c_void_p, C.c_double, C.c_int, C.c_longlong
+        L.ref_tree_build.argtypes = [i, vp, d, i, d, d]
+        L.ref_tree_build.restype = vp
+        L.ref_tree_free.argtypes = [vp]
+        for f in ["ref_tree_levels", "ref_tree_order", "ref_tree_num_nodes"]:
+            getattr(L, f).argtypes = [vp]
+            getattr(L, f).restype = i
+        L.ref_tree_nodes.argtypes = [vp] + [vp] * 7
+        L.ref_points.argtypes = [vp, C.POINTER(RefLens), ll, vp, vp, vp, vp, i]
+        if kind == "ipm":
+            L.ref_shoot_cells.argtypes = [vp, C.POINTER(RefLens), d, d, i, i, d, d, d, d, d, d, d, d, i, i, vp, vp,
+                                          vp, i]
+            L.ref_deposit_cells.argtypes = [ll, ll, vp, d, i, i, vp, vp, vp, i]
+        else:
+            L.ref_shoot_rays.argtypes = [vp, C.POINTER(RefLens), d, d, i, i, d, d, d, d, d, d, d, d, i, i, vp, vp,
+                                         vp, i]
+        _ref[kind] = L
+    return _ref[kind]
+
+
+def ref_lens(l: OrcLens) -> RefLens:
+    return RefLens(*[getattr(l, f[0]) for f in OrcLens._fields_])
+
+
+class RefTree:
+    """Tree and expansions built by the reference's own kernels on the host."""
+
+    def __init__(self, stars, root_hl, order=0, theta=1.0, alpha_error=1e-3, kind="ipm"):
+        self.L = ref_lib(kind)
+        s = np.ascontiguousarray(np.asarray(stars, np.float64).reshape(-1, 3))
+        self.h = self.L.ref_tree_build(s.shape[0], _p(s), float(root_hl), int(order), float(theta),
+                                       float(alpha_error))
+        self.levels = self.L.ref_tree_levels(self.h)
+        self.order = self.L.ref_tree_order(self.h)
+        self.n = self.L.ref_tree_num_nodes(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.ref_tree_free(self.h)
+            self.h = None
+
+    def nodes(self):
+        n, P = self.n, self.order
+        ints = np.zeros((n, 8), np.int32)
+        geom = np.zeros((n, 3))
+        nbr = np.zeros((n, 8), np.int32)
+        sil = np.zeros((n, 27), np.int32)
+        dil = np.zeros((n, 5), np.int32)
+        mult = np.zeros((n, P + 1, 2))
+        loc = np.zeros((n, P + 1, 2))
+        self.L.ref_tree_nodes(self.h, _p(ints), _p(geom), _p(nbr), _p(sil), _p(dil), _p(mult), _p(loc))
+        return ints, geom, nbr, sil, dil, mult[..., 0] + 1j * mult[..., 1], loc[..., 0] + 1j * loc[..., 1]
+
+    def points(self, lens_, zx, zy, threads=0):
+        zx = np.ascontiguousarray(zx, np.float64).ravel()
+        zy = np.ascontiguousarray(zy, np.float64).ravel()
+        wx, wy = np.zeros_like(zx), np.zeros_like(zy)
+        self.L.ref_points(self.h, C.byref(ref_lens(lens_)), zx.size, _p(zx), _p(zy), _p(wx), _p(wy), threads)
+        return wx, wy
+
+    def shoot(self, lens_, rhs, nrt, center_x, hlx, center_y, hly, npix, threads=0, parities=False, ints=False):
+        T = np.int32 if ints else np.float64
+        pix = np.zeros((npix[1], npix[0]), T)
+        pmin = np.zeros_like(pix) if parities else None
+        psad = np.zeros_like(pix) if parities else None
+        f = self.L.ref_shoot_rays if ints else self.L.ref_shoot_cells
+        f(self.h, C.byref(ref_lens(lens_)), rhs[0], rhs[1], int(nrt[0]), int(nrt[1]), center_x[0], center_x[1],
+          hlx[0], hlx[1], center_y[0], center_y[1], hly[0], hly[1], int(npix[0]), int(npix[1]), _p(pix),
+          _p(pmin) if parities else None, _p(psad) if parities else None, threads)
+        if parities and not ints:
+            pix = pmin + psad  # add_arrays_kernel (ipm.cuh:937-945)
+        return (pix, pmin, psad) if parities else pix
+
+
+def ref_deposit_cells(verts, factor, npix, parities=False):
+    L = ref_lib("ipm")
+    v = np.ascontiguousarray(verts, np.float64)
+    assert v.ndim == 3 and v.shape[2] == 2, "verts must be (ny+1, nx+1, 2)"
+    ncy, ncx = v.shape[0] - 1, v.shape[1] - 1
+    pix = np.zeros((npix[1], npix[0]))
+    pmin, psad = np.zeros_like(pix), np.zeros_like(pix)
+    L.ref_deposit_cells(ncx, ncy, _p(v), float(factor), npix[0], npix[1], _p(pix), _p(pmin), _p(psad),
+                        int(parities))
+    return (pmin + psad, pmin, psad) if parities else pix

@@ -44,7 +44,10 @@ def test_tree_structure_and_coefficients(gpu, dbl):
     assert m.value("tree_levels") == t.levels
     assert gi.shape == oi.shape
     np.testing.assert_array_equal(gi, oi)
-    np.testing.assert_array_equal(gg, og)
+    if dbl:
+        np.testing.assert_array_equal(gg, og)
+    else:  # float objects build the tree in float, as lib_ipm.so does (centres differ by float rounding)
+        np.testing.assert_allclose(gg, og, rtol=2e-7, atol=1e-6)
     for k in range(gi.shape[0]):
         assert list(gn[k, :gi[k, 5]]) == list(on[k, :oi[k, 5]])
         assert list(gs[k, :gi[k, 6]]) == list(os_[k, :oi[k, 6]])
@@ -54,8 +57,9 @@ def test_tree_structure_and_coefficients(gpu, dbl):
     om, ol = t.coeffs()
     scale_m = np.abs(om).max()
     scale_l = np.abs(ol).max()
-    assert np.abs(gm - om).max() <= 1e-9 * scale_m
-    assert np.abs(gl - ol).max() <= 1e-9 * scale_l
+    tol = 1e-9 if dbl else 1e-6  # float objects carry float node centres into the FP64 expansions
+    assert np.abs(gm - om).max() <= tol * scale_m
+    assert np.abs(gl - ol).max() <= tol * scale_l
 
 
 def _vertex_positions_oracle(m, t):
@@ -163,8 +167,15 @@ def test_irs_fp64_parities_match_oracle(gpu):
     np.testing.assert_array_equal(m.magnifications, m.magnifications_minima + m.magnifications_saddles)
 
 
+def test_irs_fp32_matches_fp64_same_expansion(gpu):
+    a = _run(irs_b200.IRS, IRS_SMALL, False, expansion_order=10)
+    b = _run(irs_b200.IRS, IRS_SMALL, True, expansion_order=10)
+    moved = np.abs(a.magnifications.astype(np.int64) - b.magnifications).sum() / 2
+    assert moved <= 2e-5 * b.num_rays_received
+
+
 def test_irs_fp32_accuracy_vs_fp64_direct(gpu):
-    m = _run(irs_b200.IRS, IRS_SMALL, False, expansion_order=10)
+    m = _run(irs_b200.IRS, IRS_SMALL, False, expansion_order=16)
     x, y = lattice(m, vertices=False)
     X, Y = np.meshgrid(x, y)
     wx, wy = po.shoot_direct(m.stars.astype(np.float64), oracle_lens(m), X, Y)
