@@ -329,6 +329,36 @@ def our_arm(args):
                 "frac": achieved / peak, "traffic": None,
                 "algorithmic": f"16 B x {nverts} corner positions + 8 B x {npix} map words"}
 
+    # ---- secondary measurements (not the headline): the plain FP64 form of the
+    # same IPM workload, and IRS on the plain-IRS case in both forms
+    extra = {}
+    if not args.no_extra:
+        plain = make_ipm(is_double=True, size=args.size)
+        plain.set_stars(stars.astype(np.float64), rectangular=False, corner=(m.value("rad"), 0.0),
+                        theta_star=m.theta_star)
+        plain.safety_scale = 1.3
+        plain.run()
+        tp = [plain.rerun(1) for _ in range(max(2, args.steps // 2))]
+        extra["ipm_fp64_plain"] = {"pixels_per_s": npix / float(np.mean(tp)), "ms_per_step": float(np.mean(tp)) * 1e3,
+                                   "lattice_ms": plain.value("t_lattice") * 1e3,
+                                   "deposit_ms": plain.value("t_deposit") * 1e3}
+        extra["ipm_fp32_over_fp64"] = float(np.mean(tp)) / (dev_time / args.steps)
+        plain.close()
+        import irs_b200
+        irs_cfg = dict(kappa_tot=0.4, shear=0.3, kappa_star=0.4, theta_star=1.0, mass_function="equal",
+                       half_length_y1=10.0, half_length_y2=10.0, num_pixels_y1=500, num_pixels_y2=500,
+                       num_rays_y=100, light_loss=0.01, random_seed=1, expansion_order=8, write_stars=0,
+                       write_maps=0, write_histograms=0)
+        for dbl, key in [(False, "irs_case1_fp32"), (True, "irs_case1_fp64_plain")]:
+            r = irs_b200.IRS(**irs_cfg, is_double=dbl)
+            r.run()
+            ts = [r.rerun(1) for _ in range(3)]
+            rays = r.num_rays_shot
+            extra[key] = {"rays_per_s": rays / float(np.mean(ts)), "rays": int(rays), "stars": int(r.num_stars),
+                          "ms_per_step": float(np.mean(ts)) * 1e3, "shoot_ms": r.value("t_lattice") * 1e3,
+                          "rays_received": int(r.num_rays_received)}
+            r.close()
+
     if rank == 0:
         cpu = cpu_baseline(m, stars.astype(np.float64), os.cpu_count() or 1) if (ws == 1 and not args.no_cpu) else None
         out = {
@@ -347,6 +377,7 @@ def our_arm(args):
             "gpu_launches": launches,
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "secondary": extra,
         }
         print(json.dumps(out))
     if dist is not None:
@@ -361,6 +392,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
     ap.add_argument("--size", default="full", choices=["full", "small"],
                     help="small: 500 x 500 map at the same pixel scale (for profiler captures)")
     args = ap.parse_args()

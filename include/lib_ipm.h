@@ -109,6 +109,8 @@ void set_stars(IPMHandle* self, const IPM_DTYPE* xym, int n, int rectangular, IP
                IPM_DTYPE corner_x2, IPM_DTYPE theta);
 double get_t_pipeline(IPMHandle* self);               /* seconds: tree + expansions + shoot */
 bool rerun(IPMHandle* self, int repeats, double* seconds); /* re-run tree+expansions+shoot on the resident stars */
+void set_band(IPMHandle* self, long long first, long long last); /* lattice row band [first, last); last < 0: all */
+bool copy_maps_device(IPMHandle* self, void* total, void* minima, void* saddles); /* integer maps to device buffers */
 bool derive(IPMHandle* self);                          /* validate + derived parameters, no GPU work */
 double get_value(IPMHandle* self, const char* name);   /* derived / run-time value by name, NaN if unknown */
 /* diagnostics: copies of internal device state */

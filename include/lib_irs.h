@@ -101,6 +101,8 @@ void set_stars(IRSHandle* self, const IRS_DTYPE* xym, int n, int rectangular, IR
                IRS_DTYPE corner_x2, IRS_DTYPE theta);
 double get_t_pipeline(IRSHandle* self);
 bool rerun(IRSHandle* self, int repeats, double* seconds); /* re-run tree+expansions+shoot on the resident stars */
+void set_band(IRSHandle* self, long long first, long long last); /* lattice row band [first, last); last < 0: all */
+bool copy_maps_device(IRSHandle* self, void* total, void* minima, void* saddles); /* integer maps to device buffers */
 bool derive(IRSHandle* self);
 double get_value(IRSHandle* self, const char* name);
 int get_tree_num_nodes(IRSHandle* self);

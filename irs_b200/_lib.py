@@ -40,7 +40,7 @@ REFERENCE_IPM_SYMBOLS = (
 )
 EXTENSION_SYMBOLS = [
     "destroy", "set_expansion_order", "get_expansion_order", "set_precision", "get_precision",
-    "set_stars", "get_t_pipeline", "rerun", "derive", "get_value", "get_tree_num_nodes", "copy_tree",
+    "set_stars", "get_t_pipeline", "rerun", "set_band", "copy_maps_device", "derive", "get_value", "get_tree_num_nodes", "copy_tree",
     "copy_coeffs", "get_num_vertices", "copy_vertices", "copy_fixed_maps",
 ]
 IRS_ONLY_SYMBOLS = ["get_t_shoot_rays", "get_num_rays_shot", "get_num_rays_received"]
@@ -122,6 +122,10 @@ def _bind(lib, kind: str, is_double: bool):
     lib.get_t_pipeline.restype = C.c_double
     lib.rerun.argtypes = [vp, C.c_int, C.POINTER(C.c_double)]
     lib.rerun.restype = C.c_bool
+    lib.set_band.argtypes = [vp, C.c_longlong, C.c_longlong]
+    lib.set_band.restype = None
+    lib.copy_maps_device.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.copy_maps_device.restype = C.c_bool
     lib.derive.argtypes = [vp]
     lib.derive.restype = C.c_bool
     lib.get_value.argtypes = [vp, C.c_char_p]

@@ -180,6 +180,19 @@ double get_value(Obj* self, const char* name) {
   return std::numeric_limits<double>::quiet_NaN();
 }
 
+// Row band [first, last) of the lattice computed by this object (rays for IRS,
+// cells for IPM); last < 0: all rows. With the integer maps of all bands
+// summed, the map equals the one-object map exactly.
+void set_band(Obj* self, long long first, long long last) {
+  self->band_lo = first;
+  self->band_hi = last;
+}
+// Integer maps into caller-provided device buffers: IPM uint64 fixed point
+// (2^32 per unit), IRS int32 counts; minima/saddles only with parities.
+bool copy_maps_device(Obj* self, void* total, void* minima, void* saddles) {
+  return self->copy_maps_device(total, minima, saddles);
+}
+
 // ---------------------------------------------------------------- diagnostics
 int get_tree_num_nodes(Obj* self) { return self->tree_num_nodes(); }
 bool copy_tree(Obj* self, int* ints, double* geom, int* nbr, int* sil, int* dil) {

@@ -42,6 +42,9 @@ class MapMaker {
   using Pix = typename std::conditional<IS_IRS, int, T>::type;
   Params<T> prm;
   int precision = kPrecisionDefault;
+  // lattice row band [band_lo, band_hi) of this object (rays for IRS, cells for
+  // IPM); band_hi < 0 means all rows. Used to split one map over several GPUs.
+  long long band_lo = 0, band_hi = -1;
   // host-provided star field (extension): used instead of generation / star file
   std::vector<StarRec<T>> host_stars;
   bool use_host_stars = false;
@@ -357,6 +360,21 @@ class MapMaker {
   bool copy_vertices(double* out) {
     return IRSB_CK(cudaMemcpy(out, d_verts_.p, d_verts_.n * sizeof(double2), cudaMemcpyDeviceToHost));
   }
+  // Integer maps copied to caller-provided device buffers (row band reduction):
+  // IPM fixed point (uint64), IRS counts (int32). min/sad only with parities.
+  bool copy_maps_device(void* total, void* mn, void* sd) {
+    const size_t n = size_t(prm.num_pixels_y.re) * prm.num_pixels_y.im;
+    const size_t es = IS_IRS ? sizeof(int) : sizeof(unsigned long long);
+    const void* a = IS_IRS ? (const void*)d_pix_.p : (const void*)d_acc_.p;
+    const void* b = IS_IRS ? (const void*)d_pmin_.p : (const void*)d_acc_min_.p;
+    const void* c = IS_IRS ? (const void*)d_psad_.p : (const void*)d_acc_sad_.p;
+    if (total && (IS_IRS || !have_parities) && !IRSB_CK(cudaMemcpyAsync(total, a, n * es, cudaMemcpyDeviceToDevice, stream_)))
+      return false;
+    if (have_parities && mn && !IRSB_CK(cudaMemcpyAsync(mn, b, n * es, cudaMemcpyDeviceToDevice, stream_))) return false;
+    if (have_parities && sd && !IRSB_CK(cudaMemcpyAsync(sd, c, n * es, cudaMemcpyDeviceToDevice, stream_))) return false;
+    return IRSB_CK(cudaStreamSynchronize(stream_));
+  }
+
   // IPM fixed-point accumulators (2^32 per unit); min/sad only with parities
   bool copy_fixed_maps(unsigned long long* total, unsigned long long* mn, unsigned long long* sd) {
     const size_t n = size_t(prm.num_pixels_y.re) * prm.num_pixels_y.im;
@@ -425,11 +443,13 @@ class MapMaker {
     sp.rhs_y = double(p.ray_half_sep.im);
     double ox = double(p.center_x.re) - double(p.half_length_x.re);
     double oy = double(p.center_x.im) - double(p.half_length_x.im);
+    sp.jbase = 0;
     if (vertices) {
       sp.base_x = ox;
       sp.base_y = oy;
       sp.nx = (long long)p.num_ray_threads.re + 1;
       sp.ny = (long long)p.num_ray_threads.im + 1;
+      sp.jbase = band_rows().first;
     } else {
       sp.base_x = ox + sp.rhs_x;
       sp.base_y = oy + sp.rhs_y;
@@ -437,6 +457,14 @@ class MapMaker {
       sp.ny = p.num_ray_threads.im;
     }
     return sp;
+  }
+
+  // [first, last) lattice rows of this object's band (rays or cells).
+  std::pair<long long, long long> band_rows() const {
+    long long n = prm.num_ray_threads.im;
+    long long lo = std::max(0LL, std::min(band_lo, n));
+    long long hi = band_hi < 0 ? n : std::max(lo, std::min(band_hi, n));
+    return {lo, hi};
   }
 
   LeafPtrs leaf_ptrs() const {
@@ -501,8 +529,11 @@ class MapMaker {
     const bool par = p.write_parities != 0;
     have_parities = par;
     ShootParams sp = shoot_params(!IS_IRS);
-    if (!build_lattice_tiles<T>(tiles_, leaves_, tree_, sp.base_x, sp.base_y, sp.rhs_x, sp.rhs_y, sp.nx, sp.ny,
-                                stream_))
+    const auto band = band_rows();
+    // rays: rows [lo, hi); cells: rows [lo, hi) need corner rows [lo, hi]
+    const long long jlo = band.first, jhi = IS_IRS ? band.second : band.second + 1;
+    if (!build_lattice_tiles<T>(tiles_, leaves_, tree_, sp.base_x, sp.base_y, sp.rhs_x, sp.rhs_y, sp.nx, sp.ny, jlo,
+                                jhi, stream_))
       return false;
     num_tiles = tiles_.total;
     launches += 4;
@@ -517,9 +548,9 @@ class MapMaker {
       }
       IRSB_CKR(cudaEventRecord(ev1_, stream_));
       if (!launch_shoot<false>(sp, d_pix_.p, d_pmin_.p, d_psad_.p, nullptr)) return false;
-      num_rays_shot = (unsigned long long)p.num_ray_threads.re * (unsigned long long)p.num_ray_threads.im;
+      num_rays_shot = (unsigned long long)p.num_ray_threads.re * (unsigned long long)(band.second - band.first);
     } else {
-      const long long nverts = sp.nx * sp.ny;
+      const long long nverts = sp.nx * (band.second - band.first + 1);
       if (!d_verts_.alloc_exact(nverts)) return false;
       const long long ndiff = (long long)p.num_pixels_y.im * (p.num_pixels_y.re + 1);
       if (!d_acc_.alloc_exact(npix) || !d_map_.alloc_exact(npix) || !d_diff_.alloc_exact(ndiff)) return false;
@@ -537,7 +568,7 @@ class MapMaker {
       }
       DepositMaps mt{d_acc_.p, d_diff_.p}, mmin{d_acc_min_.p, d_diff_min_.p}, msad{d_acc_sad_.p, d_diff_sad_.p};
       if (!launch_shoot<true>(sp, nullptr, nullptr, nullptr, d_verts_.p)) return false;
-      const long long ncx = p.num_ray_threads.re, ncy = p.num_ray_threads.im;
+      const long long ncx = p.num_ray_threads.re, ncy = band.second - band.first;
       long long ncells = ncx * ncy;
       int grid = int(std::max<long long>(1, std::min<long long>((ncells + 255) / 256, 148LL * 16)));
       if (use_fp32()) {

@@ -140,13 +140,17 @@ __device__ __forceinline__ long long lattice_lower_bound(double base, double rhs
 __global__ void leaf_rects(int nleaves, const int* __restrict__ leaf_node, const double* __restrict__ lox,
                            const double* __restrict__ hix, const double* __restrict__ loy,
                            const double* __restrict__ hiy, double base_x, double base_y, double rhs_x, double rhs_y,
-                           long long nx, long long ny, int tx, int ty, int4* rect, long long* tiles) {
+                           long long nx, long long ny, long long jlo, long long jhi, int tx, int ty, int4* rect,
+                           long long* tiles) {
   for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < nleaves; l += gridDim.x * blockDim.x) {
     int k = leaf_node[l];
     long long i0 = lattice_lower_bound(base_x, rhs_x, nx, lox[k]);
     long long i1 = lattice_lower_bound(base_x, rhs_x, nx, hix[k]);
     long long j0 = lattice_lower_bound(base_y, rhs_y, ny, loy[k]);
     long long j1 = lattice_lower_bound(base_y, rhs_y, ny, hiy[k]);
+    j0 = j0 < jlo ? jlo : j0;  // restrict to the row band [jlo, jhi)
+    j1 = j1 > jhi ? jhi : j1;
+    if (j1 < j0) j1 = j0;
     rect[l] = make_int4(int(i0), int(i1), int(j0), int(j1));
     long long ni = i1 - i0, nj = j1 - j0;
     tiles[l] = (ni > 0 && nj > 0) ? ((ni + tx - 1) / tx) * ((nj + ty - 1) / ty) : 0;
@@ -189,11 +193,12 @@ bool build_leaves(LeafSet& L, TreeDev<T>& t, FmmDev& f, const StarRec<T>* stars,
 
 template <typename T>
 bool build_lattice_tiles(LatticeTiles& W, const LeafSet& L, TreeDev<T>& t, double base_x, double base_y,
-                         double rhs_x, double rhs_y, long long nx, long long ny, cudaStream_t s) {
+                         double rhs_x, double rhs_y, long long nx, long long ny, long long jlo, long long jhi,
+                         cudaStream_t s) {
   if (!W.rect.alloc_exact(L.n) || !W.tiles.alloc_exact(L.n) || !W.tile_off.alloc_exact(L.n + 1)) return false;
   int blocks = std::max(1, std::min(ceil_div(L.n, 256), 148 * 8));
   leaf_rects<<<blocks, 256, 0, s>>>(L.n, L.node.p, t.lox.p, t.hix.p, t.loy.p, t.hiy.p, base_x, base_y, rhs_x, rhs_y,
-                                    nx, ny, kTileX, kTileY, W.rect.p, W.tiles.p);
+                                    nx, ny, jlo, jhi, kTileX, kTileY, W.rect.p, W.tiles.p);
   IRSB_LAUNCH_CK("leaf_rects");
   if (!exclusive_scan<long long>(W.tiles.p, L.n, W.tile_off.p, W.scan, s)) return false;
   IRSB_CKR(cudaMemcpyAsync(W.tile_off.p + L.n, W.scan.sum.p, sizeof(long long), cudaMemcpyDeviceToDevice, s));

@@ -50,6 +50,7 @@ struct ShootParams {
   double base_x, base_y;  // lattice coordinate of index 0
   double rhs_x, rhs_y;    // half spacing of the lattice
   long long nx, ny;       // lattice extent
+  long long jbase;        // first lattice row held in the corner buffer (row bands)
 };
 
 struct LeafPtrs {
@@ -182,7 +183,7 @@ __global__ void __launch_bounds__(kShootThreads) shoot_f64(ShootParams sp, LeafP
           w.im -= sp.cy_im;
           double px = (w.re + sp.hly_re) * sp.npx / (2.0 * sp.hly_re);
           double py = (w.im + sp.hly_im) * sp.npy / (2.0 * sp.hly_im);
-          verts[(size_t)j * (sp.nx) + i] = make_double2(px, double(sp.npy) - py);
+          verts[(size_t)(j - sp.jbase) * (sp.nx) + i] = make_double2(px, double(sp.npy) - py);
         } else {
           if (isnan(w.re) || isnan(w.im)) continue;
           w.re -= sp.cy_re;
@@ -335,7 +336,7 @@ __global__ void __launch_bounds__(kShootThreads) shoot_f32(ShootParams sp, LeafP
           py += (-a_sm.im - sp.kstar * z.im) * scy;
         }
         if (VERT) {
-          verts[(size_t)j * (sp.nx) + i] = make_double2(px, double(sp.npy) - py);
+          verts[(size_t)(j - sp.jbase) * (sp.nx) + i] = make_double2(px, double(sp.npy) - py);
         } else {
           if (!(px >= 0.0 && px <= double(sp.npx) && py >= 0.0 && py <= double(sp.npy))) continue;
           bool pmin_ = false;

@@ -970,234 +970,26 @@ void orc_ipm_deposit_ref(long long ncx, long long ncy, const double* vx, const d
 
 /* ------------------------------------------------------------ IPM, fixed-point variant */
 #define FIXSCALE 4294967296.0
-#define DEFINE_FIX(D, SUF, RINT)                                                                           \
-  typedef struct {                                                                                         \
-    D x[7], y[7];                                                                                          \
-    int n;                                                                                                 \
-  } FP_##SUF;                                                                                              \
-  static void fp_add_##SUF(FP_##SUF* p, D x, D y) {                                                        \
-    if (p->n >= 7) {                                                                                       \
-      p->n = 0;                                                                                            \
-      return;                                                                                              \
-    }                                                                                                      \
-    p->x[p->n] = x;                                                                                        \
-    p->y[p->n] = y;                                                                                        \
-    p->n++;                                                                                                \
-  }                                                                                                        \
-  static D fp_area_##SUF(const FP_##SUF* p) {                                                              \
-    if (p->n < 3) return (D)0;                                                                             \
-    D s = (D)0;                                                                                            \
-    for (int i = 0; i < p->n; i++) {                                                                       \
-      int j = (i + 1 == p->n) ? 0 : i + 1;                                                                 \
-      D dx = p->x[j] - p->x[i];                                                                            \
-      D dy = p->y[j] - p->y[i];                                                                            \
-      D t1 = dy * p->x[i];                                                                                 \
-      D t2 = dx * p->y[i];                                                                                 \
-      D t3 = t1 - t2;                                                                                      \
-      s = s + t3;                                                                                          \
-    }                                                                                                      \
-    return s / (D)2;                                                                                       \
-  }                                                                                                        \
-  static D fp_minx_##SUF(const FP_##SUF* p) {                                                              \
-    D m = p->x[0];                                                                                         \
-    for (int i = 1; i < p->n; i++) m = p->x[i] < m ? p->x[i] : m;                                          \
-    return m;                                                                                              \
-  }                                                                                                        \
-  static D fp_maxx_##SUF(const FP_##SUF* p) {                                                              \
-    D m = p->x[0];                                                                                         \
-    for (int i = 1; i < p->n; i++) m = p->x[i] > m ? p->x[i] : m;                                          \
-    return m;                                                                                              \
-  }                                                                                                        \
-  static D fp_miny_##SUF(const FP_##SUF* p) {                                                              \
-    D m = p->y[0];                                                                                         \
-    for (int i = 1; i < p->n; i++) m = p->y[i] < m ? p->y[i] : m;                                          \
-    return m;                                                                                              \
-  }                                                                                                        \
-  static D fp_maxy_##SUF(const FP_##SUF* p) {                                                              \
-    D m = p->y[0];                                                                                         \
-    for (int i = 1; i < p->n; i++) m = p->y[i] > m ? p->y[i] : m;                                          \
-    return m;                                                                                              \
-  }                                                                                                        \
-  static D fp_lerp_##SUF(D X, D x1, D y1, D x2, D y2) {                                                    \
-    D a = X - x1;                                                                                          \
-    D b = y2 - y1;                                                                                         \
-    D c = a * b;                                                                                           \
-    D d = x2 - x1;                                                                                         \
-    D e = c / d;                                                                                           \
-    return y1 + e;                                                                                         \
-  }                                                                                                        \
-  static void fp_clipx_##SUF(const FP_##SUF* P, D X, FP_##SUF* lo, FP_##SUF* hi) {                         \
-    lo->n = hi->n = 0;                                                                                     \
-    for (int i = 0; i < P->n; i++) {                                                                       \
-      int j = (i + 1 == P->n) ? 0 : i + 1;                                                                 \
-      D xi = P->x[i], yi = P->y[i];                                                                        \
-      if (xi < X) {                                                                                        \
-        fp_add_##SUF(lo, xi, yi);                                                                          \
-        if (P->x[j] > X) {                                                                                 \
-          D v = fp_lerp_##SUF(X, xi, yi, P->x[j], P->y[j]);                                                \
-          fp_add_##SUF(lo, X, v);                                                                          \
-          fp_add_##SUF(hi, X, v);                                                                          \
-        }                                                                                                  \
-      } else if (xi > X) {                                                                                 \
-        fp_add_##SUF(hi, xi, yi);                                                                          \
-        if (P->x[j] < X) {                                                                                 \
-          D v = fp_lerp_##SUF(X, xi, yi, P->x[j], P->y[j]);                                                \
-          fp_add_##SUF(lo, X, v);                                                                          \
-          fp_add_##SUF(hi, X, v);                                                                          \
-        }                                                                                                  \
-      } else {                                                                                             \
-        fp_add_##SUF(lo, xi, yi);                                                                          \
-        fp_add_##SUF(hi, xi, yi);                                                                          \
-      }                                                                                                    \
-    }                                                                                                      \
-  }                                                                                                        \
-  static void fp_clipy_##SUF(const FP_##SUF* P, D Y, FP_##SUF* lo, FP_##SUF* hi) {                         \
-    lo->n = hi->n = 0;                                                                                     \
-    for (int i = 0; i < P->n; i++) {                                                                       \
-      int j = (i + 1 == P->n) ? 0 : i + 1;                                                                 \
-      D xi = P->x[i], yi = P->y[i];                                                                        \
-      if (yi < Y) {                                                                                        \
-        fp_add_##SUF(lo, xi, yi);                                                                          \
-        if (P->y[j] > Y) {                                                                                 \
-          D v = fp_lerp_##SUF(Y, yi, xi, P->y[j], P->x[j]);                                                \
-          fp_add_##SUF(lo, v, Y);                                                                          \
-          fp_add_##SUF(hi, v, Y);                                                                          \
-        }                                                                                                  \
-      } else if (yi > Y) {                                                                                 \
-        fp_add_##SUF(hi, xi, yi);                                                                          \
-        if (P->y[j] < Y) {                                                                                 \
-          D v = fp_lerp_##SUF(Y, yi, xi, P->y[j], P->x[j]);                                                \
-          fp_add_##SUF(lo, v, Y);                                                                          \
-          fp_add_##SUF(hi, v, Y);                                                                          \
-        }                                                                                                  \
-      } else {                                                                                             \
-        fp_add_##SUF(lo, xi, yi);                                                                          \
-        fp_add_##SUF(hi, xi, yi);                                                                          \
-      }                                                                                                    \
-    }                                                                                                      \
-  }                                                                                                        \
-  static void fp_fix_##SUF(uint64_t* map, long long idx, D a, D scale) {                                   \
-    D v = a * scale;                                                                                       \
-    long long q = RINT(v);                                                                                 \
-    map[idx] += (uint64_t)q;                                                                               \
-  }                                                                                                        \
-  static D fp_abs_##SUF(D a) { return a < (D)0 ? -a : a; }                                                 \
-  static void fp_tri_##SUF(double ax, double ay, double bx, double by, double cx_, double cy_, D factor,  \
-                           int npx, int npy, uint64_t* mt, uint64_t* mmin, uint64_t* msad, int parities) { \
-    if (isnan(ax) || isnan(ay) || isnan(bx) || isnan(by) || isnan(cx_) || isnan(cy_)) return;              \
-    double fx = floor(fmin(ax, fmin(bx, cx_)));                                                            \
-    double fy = floor(fmin(ay, fmin(by, cy_)));                                                            \
-    if (!(fx > -2.0e9 && fx < 2.0e9 && fy > -2.0e9 && fy < 2.0e9)) return;                                 \
-    long long ox = (long long)fx, oy = (long long)fy;                                                      \
-    FP_##SUF P, lo, hi;                                                                                    \
-    P.n = 3;                                                                                               \
-    P.x[0] = (D)(ax - fx);                                                                                 \
-    P.y[0] = (D)(ay - fy);                                                                                 \
-    P.x[1] = (D)(bx - fx);                                                                                 \
-    P.y[1] = (D)(by - fy);                                                                                 \
-    P.x[2] = (D)(cx_ - fx);                                                                                \
-    P.y[2] = (D)(cy_ - fy);                                                                                \
-    D A = fp_area_##SUF(&P);                                                                               \
-    D lim = (D)10000 * factor;                                                                             \
-    if (!(fp_abs_##SUF(A) < lim)) return;                                                                  \
-    uint64_t* map = parities ? (A < (D)0 ? mmin : msad) : mt;                                              \
-    D X0 = (D)(-ox), X1 = (D)(npx - ox), Y0 = (D)(-oy), Y1 = (D)(npy - oy);                                \
-    if (fp_minx_##SUF(&P) >= X1 || fp_maxx_##SUF(&P) <= X0 || fp_miny_##SUF(&P) >= Y1 ||                   \
-        fp_maxy_##SUF(&P) <= Y0)                                                                           \
-      return;                                                                                              \
-    D whole = fp_abs_##SUF(A);                                                                             \
-    if (whole == (D)0) return;                                                                             \
-    D num = factor * (D)FIXSCALE;                                                                          \
-    D scale = num / whole;                                                                                 \
-    if (fp_minx_##SUF(&P) < X0) {                                                                          \
-      fp_clipx_##SUF(&P, X0, &lo, &hi);                                                                    \
-      P = hi;                                                                                              \
-    }                                                                                                      \
-    if (P.n >= 1 && fp_maxx_##SUF(&P) > X1) {                                                              \
-      fp_clipx_##SUF(&P, X1, &lo, &hi);                                                                    \
-      P = lo;                                                                                              \
-    }                                                                                                      \
-    if (P.n >= 1 && fp_miny_##SUF(&P) < Y0) {                                                              \
-      fp_clipy_##SUF(&P, Y0, &lo, &hi);                                                                    \
-      P = hi;                                                                                              \
-    }                                                                                                      \
-    if (P.n >= 1 && fp_maxy_##SUF(&P) > Y1) {                                                              \
-      fp_clipy_##SUF(&P, Y1, &lo, &hi);                                                                    \
-      P = lo;                                                                                              \
-    }                                                                                                      \
-    if (P.n < 3) return;                                                                                   \
-    uint64_t qfull = (uint64_t)RINT(scale);                                                                \
-    int ymin = (int)fp_miny_##SUF(&P), ymax = (int)fp_maxy_##SUF(&P);                                      \
-    if (ymax + oy == npy) ymax--;                                                                          \
-    for (int y = ymin; y <= ymax; y++) {                                                                   \
-      FP_##SUF S;                                                                                          \
-      if (y < ymax) {                                                                                      \
-        fp_clipy_##SUF(&P, (D)(y + 1), &S, &hi);                                                           \
-        P = hi;                                                                                            \
-      } else {                                                                                             \
-        S = P;                                                                                             \
-      }                                                                                                    \
-      if (S.n < 3) continue;                                                                               \
-      long long row = oy + y;                                                                              \
-      D yb = (D)y, yt = (D)(y + 1);                                                                        \
-      D b0 = 0, b1 = 0, t0 = 0, t1 = 0;                                                                    \
-      int hb = 0, ht = 0;                                                                                  \
-      for (int i = 0; i < S.n; i++) {                                                                      \
-        D vx = S.x[i], vy = S.y[i];                                                                        \
-        if (vy == yb) {                                                                                    \
-          b0 = hb ? (vx < b0 ? vx : b0) : vx;                                                              \
-          b1 = hb ? (vx > b1 ? vx : b1) : vx;                                                              \
-          hb = 1;                                                                                          \
-        }                                                                                                  \
-        if (vy == yt) {                                                                                    \
-          t0 = ht ? (vx < t0 ? vx : t0) : vx;                                                              \
-          t1 = ht ? (vx > t1 ? vx : t1) : vx;                                                              \
-          ht = 1;                                                                                          \
-        }                                                                                                  \
-      }                                                                                                    \
-      int xa = 1, xb = 0;                                                                                  \
-      if (hb && ht) {                                                                                      \
-        D l = b0 > t0 ? b0 : t0, r = b1 < t1 ? b1 : t1;                                                    \
-        xa = (int)ceil((double)l);                                                                         \
-        xb = (int)floor((double)r);                                                                        \
-      }                                                                                                    \
-      int xmin = (int)fp_minx_##SUF(&S), xmax = (int)fp_maxx_##SUF(&S);                                    \
-      if (xmax + ox == npx) xmax--;                                                                        \
-      FP_##SUF R = S;                                                                                      \
-      int x = xmin;                                                                                        \
-      while (x < xmax) {                                                                                   \
-        if (xa < xb && x == xa) {                                                                          \
-          fp_clipx_##SUF(&R, (D)xb, &lo, &hi);                                                             \
-          R = hi;                                                                                          \
-          for (int c = xa; c < xb; c++) map[row * npx + ox + c] += qfull;                                  \
-          x = xb;                                                                                          \
-          continue;                                                                                        \
-        }                                                                                                  \
-        FP_##SUF Lp;                                                                                       \
-        fp_clipx_##SUF(&R, (D)(x + 1), &Lp, &hi);                                                          \
-        R = hi;                                                                                            \
-        if (Lp.n >= 3) fp_fix_##SUF(map, row * npx + ox + x, fp_abs_##SUF(fp_area_##SUF(&Lp)), scale);     \
-        x++;                                                                                               \
-      }                                                                                                    \
-      if (x == xmax) fp_fix_##SUF(map, row * npx + ox + xmax, fp_abs_##SUF(fp_area_##SUF(&R)), scale);     \
-    }                                                                                                      \
-  }                                                                                                        \
-  void orc_ipm_deposit_fix_##SUF(long long ncx, long long ncy, const double* vxy, D factor, int npx, int npy, \
-                                 uint64_t* mt, uint64_t* mmin, uint64_t* msad, int parities) {             \
-    long long W = ncx + 1;                                                                                 \
-    for (long long j = 0; j < ncy; j++)                                                                    \
-      for (long long i = 0; i < ncx; i++) {                                                                \
-        const double* y0 = vxy + 2 * ((j + 1) * W + i + 1);                                                \
-        const double* y1 = vxy + 2 * ((j + 1) * W + i);                                                    \
-        const double* y2 = vxy + 2 * (j * W + i);                                                          \
-        const double* y3 = vxy + 2 * (j * W + i + 1);                                                      \
-        fp_tri_##SUF(y0[0], y0[1], y1[0], y1[1], y2[0], y2[1], factor, npx, npy, mt, mmin, msad, parities); \
-        fp_tri_##SUF(y2[0], y2[1], y3[0], y3[1], y0[0], y0[1], factor, npx, npy, mt, mmin, msad, parities); \
-      }                                                                                                    \
-  }
+#define CAT2(a, b) a##_##b
+#define CAT(a, b) CAT2(a, b)
+#define FN(name) CAT(name, SUF)
+#define TRI(suf) CAT(Tri, suf)
 
-DEFINE_FIX(float, f32, llrintf)
-DEFINE_FIX(double, f64, llrint)
+#define D float
+#define SUF f32
+#define RINT llrintf
+#include "fixdep.inc"
+#undef D
+#undef SUF
+#undef RINT
+
+#define D double
+#define SUF f64
+#define RINT llrint
+#include "fixdep.inc"
+#undef D
+#undef SUF
+#undef RINT
 
 /* ------------------------------------------------------------ derived parameters (double) */
 /* calculate_derived_params, include/ipm.cuh:434-506 for a generated circular or

@@ -171,7 +171,7 @@ def test_irs_fp32_matches_fp64_same_expansion(gpu):
     a = _run(irs_b200.IRS, IRS_SMALL, False, expansion_order=10)
     b = _run(irs_b200.IRS, IRS_SMALL, True, expansion_order=10)
     moved = np.abs(a.magnifications.astype(np.int64) - b.magnifications).sum() / 2
-    assert moved <= 2e-5 * b.num_rays_received
+    assert moved <= 2e-4 * b.num_rays_received  # ~2 x FP32 position error / pixel size
 
 
 def test_irs_fp32_accuracy_vs_fp64_direct(gpu):
