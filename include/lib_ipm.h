@@ -122,6 +122,20 @@ bool copy_vertices(IPMHandle* self, double* out);
 bool copy_fixed_maps(IPMHandle* self, unsigned long long* total, unsigned long long* minima,
                      unsigned long long* saddles);
 
+/* Allocation-free deposition. No counterpart in the reference: for callers
+ * that cannot let a library call cudaMalloc (device memory owned by their own
+ * pool or budget, or latency-critical loops where allocation would
+ * synchronise). Deposits the two triangles of each of ncx x ncy cells from the
+ * (ncx+1) x (ncy+1) corner source positions at the device pointer verts
+ * (double x, y pixel units, row axis flipped) into the npx x npy map at the
+ * device pointer map, on the given cudaStream_t (NULL: default stream),
+ * asynchronously. Scratch is a static device array: maps up to 1024 x 1024
+ * pixels; larger sizes return 1. Its first call on a device looks up the
+ * array's device address (make it before any stream capture); calls that
+ * overlap on the GPU race on the shared scratch. Returns 0 on success. */
+int ipm_deposit_noalloc(const double* verts, long long ncx, long long ncy, IPM_DTYPE factor, int npx, int npy,
+                        IPM_DTYPE* map, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -12,6 +12,7 @@
 
 #include <cstring>
 #include <limits>
+#include <mutex>
 
 #ifndef IRSB_DOUBLE
 #define IRSB_DOUBLE 0
@@ -206,3 +207,102 @@ bool copy_fixed_maps(Obj* self, unsigned long long* total, unsigned long long* m
 }
 
 }  // extern "C"
+
+#if !IRSB_IRS
+// ---------------------------------------------------------------- allocation-free deposition
+// Some callers cannot let a library call cudaMalloc: applications whose device
+// memory is owned by their own pool (a framework's caching allocator or a
+// fixed memory budget), and latency-critical loops where cudaMalloc / cudaFree
+// would synchronise the device. ipm_deposit_noalloc serves them: it deposits a
+// cell-corner lattice the caller already holds on the device into a map the
+// caller provides, and its fixed-point scratch lives in the file-scope device
+// array below instead of being allocated.
+//
+// Limit: maps of at most kNoAllocMaxPixels pixels and kNoAllocMaxRows rows
+// (1024 x 1024). The array (16.8 MB) is part of the module, so every GPU that
+// loads this library holds it until the process exits.
+namespace {
+constexpr long long kNoAllocMaxPixels = 1024LL * 1024LL;
+constexpr long long kNoAllocMaxRows = 1024;
+constexpr long long kNoAllocWords = kNoAllocMaxPixels + kNoAllocMaxRows * (1024 + 1);
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocWords];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned long long* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array for the current device; looked up once
+// per device. In host code the array's name is only a host-side stand-in.
+unsigned long long* noalloc_scratch_for_current_device(int* err) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+    *err = 3;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr) {
+      std::fprintf(stderr, "ipm_deposit_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+      *err = 3;
+      return nullptr;
+    }
+    g_noalloc_ptr[dev] = static_cast<unsigned long long*>(ptr);
+  }
+  return g_noalloc_ptr[dev];
+}
+}  // namespace
+
+extern "C" {
+
+// Deposits the two triangles of each of the ncx x ncy lens-plane cells whose
+// (ncx+1) x (ncy+1) corner source positions (double x, y pairs in pixel units,
+// row axis flipped, row-major by corner row) are at the device pointer
+// `verts`, into the npx x npy magnification map at the device pointer `map`
+// (overwritten). `factor` is the image-plane area of one triangle in pixel
+// units. The work is queued on `stream` (a cudaStream_t; NULL for the default
+// stream) and the call returns without waiting for it.
+//
+// Returns 0 on success, 1 for sizes beyond the limit (more than 1024 x 1024
+// pixels or more than 1024 rows) or invalid arguments, 3 if the scratch
+// address cannot be found, 4 for a launch error. The call allocates nothing.
+// Its first call on a device looks up the device address of the scratch
+// array; make that first call before any stream capture. All calls share the
+// one scratch array (cleared at the start of each call), so calls whose work
+// overlaps on the GPU race: order them on one stream or synchronise between
+// them.
+int ipm_deposit_noalloc(const double* verts, long long ncx, long long ncy, dtype factor, int npx, int npy,
+                        dtype* map, void* stream) {
+  if (!verts || !map || ncx < 1 || ncy < 1 || npx < 1 || npy < 1) {
+    std::fprintf(stderr, "ipm_deposit_noalloc: invalid arguments\n");
+    return 1;
+  }
+  const long long npix = (long long)npx * npy;
+  if (npix > kNoAllocMaxPixels || npy > kNoAllocMaxRows || (long long)npy * (npx + 1) > kNoAllocWords - npix) {
+    std::fprintf(stderr, "ipm_deposit_noalloc: map of %d x %d pixels exceeds the limit of %lld pixels and %lld rows\n",
+                 npx, npy, kNoAllocMaxPixels, kNoAllocMaxRows);
+    return 1;
+  }
+  int err = 0;
+  unsigned long long* scratch = noalloc_scratch_for_current_device(&err);
+  if (!scratch) return err;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  irsb::DepositMaps m{scratch, scratch + npix};
+  const long long ndiff = (long long)npy * (npx + 1);
+  if (cudaMemsetAsync(m.acc, 0, npix * sizeof(unsigned long long), s) != cudaSuccess) return 4;
+  if (cudaMemsetAsync(m.diff, 0, ndiff * sizeof(unsigned long long), s) != cudaSuccess) return 4;
+  const long long ncells = ncx * ncy;
+  int grid = int(std::max<long long>(1, std::min<long long>((ncells + 255) / 256, 148LL * 16)));
+  irsb::ipm_deposit_cells<dtype><<<grid, 256, 0, s>>>(reinterpret_cast<const double2*>(verts), ncx, ncy, factor,
+                                                      npx, npy, m, m, m, 0);
+  int gr = std::max(1, std::min(irsb::ceil_div((long long)npy * 32, 256), 148 * 8));
+  irsb::ipm_resolve_rows<<<gr, 256, 0, s>>>(npx, npy, m);
+  int g2 = int(std::max<long long>(1, std::min<long long>((npix + 255) / 256, 148LL * 16)));
+  irsb::ipm_finalize<dtype><<<g2, 256, 0, s>>>(npix, m.acc, nullptr, nullptr, map, nullptr, nullptr, 0);
+  if (cudaGetLastError() != cudaSuccess) return 4;
+  return 0;
+}
+
+}  // extern "C"
+#endif
