@@ -3,6 +3,8 @@
 Produces, under irs_b200/lib/:
   lib_ipm.so, lib_ipm_double.so   IPM, float / double (reference lib_ipm.so ABI)
   lib_irs.so, lib_irs_double.so   IRS, float / double (same conventions)
+and under irs_b200/bin/ the command-line tools of the reference
+(src/main_ipm_irs.cu): ipm_gpu, ipm_gpu_double, irs_gpu, irs_gpu_double.
 
 Usage: python -m irs_b200.build [--jobs N] [--force]
 """
@@ -18,6 +20,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
+BINDIR = os.path.join(HERE, "bin")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
@@ -28,6 +31,13 @@ NVCC_FLAGS = ARCH + [
     "-shared",
     "--expt-relaxed-constexpr",
 ]
+
+EXECUTABLES = {
+    "ipm_gpu": ["-DIRSB_DOUBLE=0", "-DIRSB_IRS=0"],
+    "ipm_gpu_double": ["-DIRSB_DOUBLE=1", "-DIRSB_IRS=0"],
+    "irs_gpu": ["-DIRSB_DOUBLE=0", "-DIRSB_IRS=1"],
+    "irs_gpu_double": ["-DIRSB_DOUBLE=1", "-DIRSB_IRS=1"],
+}
 
 VARIANTS = {
     "lib_ipm.so": ["-DIRSB_DOUBLE=0", "-DIRSB_IRS=0"],
@@ -71,9 +81,27 @@ def build_one(name: str, defs, force: bool = False, extra=None) -> str:
     return out
 
 
-def build(force: bool = False, jobs: int = 4, extra=None) -> list[str]:
+def build_exe(name: str, defs, force: bool = False) -> str:
+    os.makedirs(BINDIR, exist_ok=True)
+    out = os.path.join(BINDIR, name)
+    if not force and not _stale(out):
+        return out
+    flags = [f for f in NVCC_FLAGS if f not in ("-shared",)]
+    cmd = [nvcc()] + flags + list(defs) + ["-I", CSRC, os.path.join(CSRC, "cli.cu"), "-o", out + ".tmp",
+                                            "-lcurand"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError(f"nvcc failed for {name}")
+    os.replace(out + ".tmp", out)
+    return out
+
+
+def build(force: bool = False, jobs: int = 4, extra=None, executables: bool = True) -> list[str]:
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
-        futs = {ex.submit(build_one, n, d, force, extra): n for n, d in VARIANTS.items()}
+        futs = [ex.submit(build_one, n, d, force, extra) for n, d in VARIANTS.items()]
+        if executables:
+            futs += [ex.submit(build_exe, n, d, force) for n, d in EXECUTABLES.items()]
         return [f.result() for f in cf.as_completed(futs)]
 
 

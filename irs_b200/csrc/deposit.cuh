@@ -11,8 +11,10 @@
 //
 // How, differently by design:
 //   * the overlap of a triangle with a pixel is computed directly from
-//     Green's theorem (pixel_coverage) instead of by successive polygon
-//     clips: register-only arithmetic, no polygon arrays;
+//     Green's theorem instead of by successive polygon clips: the edges are
+//     clipped once per row strip (row_geometry), and each pixel of the row
+//     then only clamps those segments to its column (pixel_coverage):
+//     register-only arithmetic, no polygon arrays;
 //   * rows of a triangle are independent work items; a warp expands the rows
 //     of its 64 triangles and shares them out 32 at a time;
 //   * pixels inside both the bottom and the top chord of a row strip are fully
@@ -28,6 +30,8 @@
 #pragma once
 #include "common.cuh"
 
+#include <limits>
+
 namespace irsb {
 
 template <typename D>
@@ -38,6 +42,7 @@ struct RN<float> {
   static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
   static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
   static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+  static __device__ __forceinline__ float rcp(float a) { return __frcp_rn(a); }
   static __device__ __forceinline__ unsigned long long to_fix(float a) {
     return (unsigned long long)__float2ll_rn(a);
   }
@@ -48,6 +53,7 @@ struct RN<double> {
   static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
   static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
   static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+  static __device__ __forceinline__ double rcp(double a) { return __drcp_rn(a); }
   static __device__ __forceinline__ unsigned long long to_fix(double a) {
     return (unsigned long long)__double2ll_rn(a);
   }
@@ -70,7 +76,8 @@ struct DepositMaps {
 template <typename D>
 struct Tri {
   D x[3], y[3];     // CCW, relative to (ox, oy)
-  D idx[3], idy[3]; // 1 / (x[k+1] - x[k]), 1 / (y[k+1] - y[k]) (0 for a zero difference)
+  D idy[3];         // 1 / (y[k+1] - y[k]) (0 for a zero difference)
+  D sl[3];          // slope (y[k+1] - y[k]) * (1 / (x[k+1] - x[k])); 0 for a vertical edge or an overflow
   D scale;          // factor * 2^32 / |area|
   int ox, oy;
   int rlo, nrows;   // first row (relative) and number of rows to visit
@@ -79,7 +86,7 @@ struct Tri {
 
 template <typename D>
 __device__ __forceinline__ D rcp_or_zero(D v) {
-  return v != D(0) ? RN<D>::div(D(1), v) : D(0);
+  return v != D(0) ? RN<D>::rcp(v) : D(0);  // correctly rounded 1 / v
 }
 
 // Triangle (a, b, c) in absolute pixel coordinates (row axis flipped) ->
@@ -95,7 +102,7 @@ __device__ __forceinline__ Tri<D> setup_triangle(double ax, double ay, double bx
   t.ox = t.oy = 0;
   t.map = 0;
   t.scale = D(0);
-  for (int k = 0; k < 3; k++) t.x[k] = t.y[k] = t.idx[k] = t.idy[k] = D(0);
+  for (int k = 0; k < 3; k++) t.x[k] = t.y[k] = t.sl[k] = t.idy[k] = D(0);
   if (isnan(ax) || isnan(ay) || isnan(bx) || isnan(by) || isnan(cx) || isnan(cy)) return t;
   double fx = floor(fmin(ax, fmin(bx, cx)));
   double fy = floor(fmin(ay, fmin(by, cy)));
@@ -134,8 +141,10 @@ __device__ __forceinline__ Tri<D> setup_triangle(double ax, double ay, double bx
   t.y[2] = y2;
   for (int k = 0; k < 3; k++) {
     int j = k == 2 ? 0 : k + 1;
-    t.idx[k] = rcp_or_zero(RN<D>::sub(t.x[j], t.x[k]));
-    t.idy[k] = rcp_or_zero(RN<D>::sub(t.y[j], t.y[k]));
+    const D dx = RN<D>::sub(t.x[j], t.x[k]), dy = RN<D>::sub(t.y[j], t.y[k]);
+    t.idy[k] = rcp_or_zero(dy);
+    const D g = RN<D>::mul(dy, rcp_or_zero(dx));
+    t.sl[k] = dabs(g) <= std::numeric_limits<D>::max() ? g : D(0);
   }
   t.scale = RN<D>::div(RN<D>::mul(factor, D(kFixScale)), whole);
   t.ox = ox;
@@ -148,72 +157,102 @@ __device__ __forceinline__ Tri<D> setup_triangle(double ax, double ay, double bx
   return t;
 }
 
-// x-extent [lo, hi] of the triangle on the horizontal line y = yk; false if it
-// does not reach that line.
+// Geometry of one row strip [rb, rt = rb + 1] of a triangle.
+//   Strip segments: each edge clipped to the strip, endpoints (xa, ya) ->
+//   (xb, yb) with y relative to rb, a zero segment where the edge misses the
+//   strip. A horizontal edge belongs to the strip only on [rb, rt), so an edge
+//   lying on the line between two rows is counted once (by the top chord of
+//   the row below).
+//   Chords: x-extent of the triangle on the lines y = rb and y = rt (an edge
+//   reaching the line contributes its crossing, x1 + ((y - y1) / dy) dx, or
+//   both ends when it lies on the line).
 template <typename D>
-__device__ __forceinline__ bool chord(const Tri<D>& t, D yk, D& lo, D& hi) {
+struct Strip {
+  D xa[3], ya[3], xb[3], yb[3];
+};
+
+template <typename D>
+__device__ __forceinline__ void extend(bool& any, D& lo, D& hi, D a, D b) {
+  const D mn = a < b ? a : b, mx = a > b ? a : b;
+  lo = any ? (mn < lo ? mn : lo) : mn;
+  hi = any ? (mx > hi ? mx : hi) : mx;
+  any = true;
+}
+
+// Fills the strip segments and both chords; returns false when the triangle
+// does not enter the strip, else sets its x-extent [xlo, xhi] there.
+template <typename D>
+__device__ __forceinline__ bool row_geometry(const Tri<D>& t, D rb, D rt, Strip<D>& g, D& xlo, D& xhi, bool& hb,
+                                             D& cb0, D& cb1, bool& ht, D& ct0, D& ct1) {
   bool any = false;
-  lo = D(0);
-  hi = D(0);
+  xlo = xhi = cb0 = cb1 = ct0 = ct1 = D(0);
+  hb = ht = false;
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     const int j = k == 2 ? 0 : k + 1;
-    const D y1 = t.y[k], y2 = t.y[j], x1 = t.x[k], x2 = t.x[j];
-    if ((y1 <= yk && yk <= y2) || (y2 <= yk && yk <= y1)) {
-      D xa, xb;
-      if (y1 != y2) {
-        xa = RN<D>::add(x1, RN<D>::mul(RN<D>::mul(RN<D>::sub(yk, y1), t.idy[k]), RN<D>::sub(x2, x1)));
-        xb = xa;
-      } else {
-        xa = x1;
-        xb = x2;
+    const D x1 = t.x[k], y1 = t.y[k], x2 = t.x[j], y2 = t.y[j];
+    const D dx = RN<D>::sub(x2, x1), dy = RN<D>::sub(y2, y1);
+    const bool on_b = (y1 <= rb && rb <= y2) || (y2 <= rb && rb <= y1);
+    const bool on_t = (y1 <= rt && rt <= y2) || (y2 <= rt && rt <= y1);
+    D t0 = D(0), t1 = D(1);
+    bool ok;
+    if (dy != D(0)) {
+      const D ta = RN<D>::mul(RN<D>::sub(rb, y1), t.idy[k]), tb = RN<D>::mul(RN<D>::sub(rt, y1), t.idy[k]);
+      if (on_b) {
+        const D p = RN<D>::add(x1, RN<D>::mul(ta, dx));
+        extend(hb, cb0, cb1, p, p);
       }
-      D mn = xa < xb ? xa : xb, mx = xa > xb ? xa : xb;
-      lo = any ? (mn < lo ? mn : lo) : mn;
-      hi = any ? (mx > hi ? mx : hi) : mx;
-      any = true;
+      if (on_t) {
+        const D p = RN<D>::add(x1, RN<D>::mul(tb, dx));
+        extend(ht, ct0, ct1, p, p);
+      }
+      const D lo = ta < tb ? ta : tb, hi = ta > tb ? ta : tb;
+      t0 = lo > t0 ? lo : t0;
+      t1 = hi < t1 ? hi : t1;
+      ok = t0 < t1;
+    } else {
+      if (on_b) extend(hb, cb0, cb1, x1, x2);
+      if (on_t) extend(ht, ct0, ct1, x1, x2);
+      ok = y1 >= rb && y1 < rt;
     }
+    D xa = D(0), ya = D(0), xb = D(0), yb = D(0);
+    if (ok) {
+      xa = RN<D>::add(x1, RN<D>::mul(t0, dx));
+      xb = RN<D>::add(x1, RN<D>::mul(t1, dx));
+      ya = RN<D>::sub(RN<D>::add(y1, RN<D>::mul(t0, dy)), rb);
+      yb = RN<D>::sub(RN<D>::add(y1, RN<D>::mul(t1, dy)), rb);
+      extend(any, xlo, xhi, xa, xb);
+    }
+    g.xa[k] = xa;
+    g.ya[k] = ya;
+    g.xb[k] = xb;
+    g.yb[k] = yb;
   }
   return any;
 }
 
-// Area of the triangle inside the pixel [c, c+1] x [r, r+1] (relative
-// coordinates) from Green's theorem, area = -sum over the boundary of
-// integral (y - r) dx: each edge contributes its segment clipped to the pixel
-// (a trapezoid), the pixel's top side contributes the chord length at y = r+1
-// inside [c, c+1], the vertical sides and the bottom side contribute nothing.
+// Area of the triangle inside the pixel [c, c+1] x [rb, rb+1] from Green's
+// theorem, area = -(sum over the boundary of the integral of (y - rb) dx):
+// each strip segment restricted to the column (both ends clamped to
+// [c, c+1], an edge being monotone in x) is a trapezoid; the pixel's top side
+// adds the top chord's length inside the column; the vertical sides and the
+// bottom side add nothing.
 template <typename D>
-__device__ __forceinline__ D pixel_coverage(const Tri<D>& t, D c, D r, bool has_top, D ct0, D ct1) {
-  const D c1 = RN<D>::add(c, D(1)), r1 = RN<D>::add(r, D(1));
+__device__ __forceinline__ D pixel_coverage(const Tri<D>& t, const Strip<D>& g, D c, bool has_top, D ct0, D ct1) {
+  const D c1 = RN<D>::add(c, D(1));
   D s = D(0);
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    const int j = k == 2 ? 0 : k + 1;
-    const D x1 = t.x[k], y1 = t.y[k];
-    const D dx = RN<D>::sub(t.x[j], x1), dy = RN<D>::sub(t.y[j], y1);
-    D t0 = D(0), t1 = D(1);
-    bool ok = true;
-    if (dx != D(0)) {
-      D ta = RN<D>::mul(RN<D>::sub(c, x1), t.idx[k]), tb = RN<D>::mul(RN<D>::sub(c1, x1), t.idx[k]);
-      D lo = ta < tb ? ta : tb, hi = ta > tb ? ta : tb;
-      t0 = lo > t0 ? lo : t0;
-      t1 = hi < t1 ? hi : t1;
-    } else {
-      ok = !(x1 < c || x1 > c1);
-    }
-    if (dy != D(0)) {
-      D ta = RN<D>::mul(RN<D>::sub(r, y1), t.idy[k]), tb = RN<D>::mul(RN<D>::sub(r1, y1), t.idy[k]);
-      D lo = ta < tb ? ta : tb, hi = ta > tb ? ta : tb;
-      t0 = lo > t0 ? lo : t0;
-      t1 = hi < t1 ? hi : t1;
-    } else {
-      ok = ok && !(y1 < r || y1 > r1);
-    }
-    if (ok && t0 < t1) {
-      const D xa = RN<D>::add(x1, RN<D>::mul(t0, dx)), xb = RN<D>::add(x1, RN<D>::mul(t1, dx));
-      const D ya = RN<D>::sub(RN<D>::add(y1, RN<D>::mul(t0, dy)), r);
-      const D yb = RN<D>::sub(RN<D>::add(y1, RN<D>::mul(t1, dy)), r);
-      s = RN<D>::sub(s, RN<D>::mul(RN<D>::mul(RN<D>::sub(xb, xa), RN<D>::add(ya, yb)), D(0.5)));
+    D xs = g.xa[k], xe = g.xb[k];
+    xs = xs > c ? xs : c;
+    xs = xs < c1 ? xs : c1;
+    xe = xe > c ? xe : c;
+    xe = xe < c1 ? xe : c1;
+    const D w = RN<D>::sub(xe, xs);
+    if (w != D(0)) {
+      const D ys = RN<D>::add(g.ya[k], RN<D>::mul(RN<D>::sub(xs, g.xa[k]), t.sl[k]));
+      const D ye = RN<D>::add(g.ya[k], RN<D>::mul(RN<D>::sub(xe, g.xa[k]), t.sl[k]));
+      s = RN<D>::sub(s, RN<D>::mul(RN<D>::mul(w, RN<D>::add(ys, ye)), D(0.5)));
     }
   }
   if (has_top) {
@@ -228,31 +267,10 @@ __device__ __forceinline__ D pixel_coverage(const Tri<D>& t, D c, D r, bool has_
 template <typename D>
 __device__ __forceinline__ void deposit_row(const Tri<D>& t, int r, int npx, DepositMaps M) {
   const D rb = D(r), rt = D(r + 1);
-  D cb0, cb1, ct0, ct1;
-  const bool hb = chord(t, rb, cb0, cb1);
-  const bool ht = chord(t, rt, ct0, ct1);
-  // x-extent of the triangle within the row
-  bool any = false;
-  D xlo = D(0), xhi = D(0);
-  if (hb) {
-    xlo = cb0;
-    xhi = cb1;
-    any = true;
-  }
-  if (ht) {
-    xlo = any ? (ct0 < xlo ? ct0 : xlo) : ct0;
-    xhi = any ? (ct1 > xhi ? ct1 : xhi) : ct1;
-    any = true;
-  }
-#pragma unroll
-  for (int k = 0; k < 3; k++) {
-    if (t.y[k] > rb && t.y[k] < rt) {
-      xlo = any ? (t.x[k] < xlo ? t.x[k] : xlo) : t.x[k];
-      xhi = any ? (t.x[k] > xhi ? t.x[k] : xhi) : t.x[k];
-      any = true;
-    }
-  }
-  if (!any) return;
+  Strip<D> g;
+  D xlo, xhi, cb0, cb1, ct0, ct1;
+  bool hb, ht;
+  if (!row_geometry(t, rb, rt, g, xlo, xhi, hb, cb0, cb1, ht, ct0, ct1)) return;
   const int cmap_lo = -t.ox, cmap_hi = npx - 1 - t.ox;  // columns inside the map (relative)
   int cmin = int(floor(xlo)), cmax = int(floor(xhi));
   if (cmin < cmap_lo) cmin = cmap_lo;
@@ -279,7 +297,7 @@ __device__ __forceinline__ void deposit_row(const Tri<D>& t, int r, int npx, Dep
       c = xb - 1;
       continue;
     }
-    D a = pixel_coverage(t, D(c), rb, ht, ct0, ct1);
+    D a = pixel_coverage(t, g, D(c), ht, ct0, ct1);
     if (a > D(0)) {
       unsigned long long q = RN<D>::to_fix(RN<D>::mul(a, t.scale));
       if (q) atomicAdd(M.acc + rbase + c, q);
@@ -288,16 +306,18 @@ __device__ __forceinline__ void deposit_row(const Tri<D>& t, int r, int npx, Dep
 }
 
 // Cells of an ncx x ncy lattice whose (ncx+1) x (ncy+1) corner positions are in
-// `verts`. A warp takes 32 consecutive cells (64 triangles), scans their row
-// counts and then works through all (triangle, row) items 32 at a time: each
-// lane finds its item's owner lane by a binary search over the scan and reads
+// `verts`. A warp takes 32 consecutive cells and handles their first
+// triangles, then their second triangles: each lane prepares one triangle and
+// deposits its first row; the warp then scans the counts of the remaining
+// rows and works through those (triangle, row) items 32 at a time, each lane
+// finding its item's owner lane by a binary search over the scan and reading
 // the triangle through shuffles, so a triangle with many rows is spread over
 // the warp instead of holding one lane.
 template <typename D>
-__global__ void __launch_bounds__(256) ipm_deposit_cells(const double2* __restrict__ verts, long long ncx,
-                                                         long long ncy, D factor, int npx, int npy,
-                                                         DepositMaps m_total, DepositMaps m_min, DepositMaps m_sad,
-                                                         int parities) {
+__global__ void __launch_bounds__(256, sizeof(D) == 4 ? 4 : 2) ipm_deposit_cells(const double2* __restrict__ verts, long long ncx,
+                                                            long long ncy, D factor, int npx, int npy,
+                                                            DepositMaps m_total, DepositMaps m_min,
+                                                            DepositMaps m_sad, int parities) {
   const long long ncells = ncx * ncy;
   const long long vx = ncx + 1;
   const int lane = threadIdx.x & 31;
@@ -305,71 +325,63 @@ __global__ void __launch_bounds__(256) ipm_deposit_cells(const double2* __restri
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   for (long long base = warp0 * 32; base < ncells; base += nwarps * 32) {
     const long long c = base + lane;
-    Tri<D> ta, tb;
-    ta.nrows = tb.nrows = 0;
+    double2 y0 = make_double2(0, 0), y1 = y0, y2 = y0, y3 = y0;
     if (c < ncells) {
       long long j = c / ncx, i = c - j * ncx;
-      double2 y0 = verts[(j + 1) * vx + (i + 1)];  // z + rhs
-      double2 y1 = verts[(j + 1) * vx + i];        // z - conj(rhs)
-      double2 y2 = verts[j * vx + i];              // z - rhs
-      double2 y3 = verts[j * vx + (i + 1)];        // z + conj(rhs)
-      ta = setup_triangle<D>(y0.x, y0.y, y1.x, y1.y, y2.x, y2.y, factor, npx, npy, parities != 0);
-      tb = setup_triangle<D>(y2.x, y2.y, y3.x, y3.y, y0.x, y0.y, factor, npx, npy, parities != 0);
+      y0 = verts[(j + 1) * vx + (i + 1)];  // z + rhs
+      y1 = verts[(j + 1) * vx + i];        // z - conj(rhs)
+      y2 = verts[j * vx + i];              // z - rhs
+      y3 = verts[j * vx + (i + 1)];        // z + conj(rhs)
     }
-    // inclusive scan of this lane's row count over the warp
-    const int mine = ta.nrows + tb.nrows;
-    int incl = mine;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int v = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += v;
-    }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    for (int it0 = 0; it0 < total; it0 += 32) {
-      const int item = it0 + lane;
-      // owner: first lane whose inclusive count exceeds item
-      int lo = 0, hi = 31;
-#pragma unroll
-      for (int step = 0; step < 5; step++) {
-        int mid = (lo + hi) >> 1;
-        int v = __shfl_sync(0xffffffffu, incl, mid);
-        if (v > item) hi = mid;
-        else lo = mid + 1;
+#pragma unroll 1
+    for (int half = 0; half < 2; half++) {
+      Tri<D> mine;
+      mine.nrows = 0;
+      if (c < ncells) {
+        mine = half == 0 ? setup_triangle<D>(y0.x, y0.y, y1.x, y1.y, y2.x, y2.y, factor, npx, npy, parities != 0)
+                         : setup_triangle<D>(y2.x, y2.y, y3.x, y3.y, y0.x, y0.y, factor, npx, npy, parities != 0);
       }
-      const int owner = lo;
-      const int before = __shfl_sync(0xffffffffu, incl - mine, owner);
-      const int na = __shfl_sync(0xffffffffu, ta.nrows, owner);
-      const int k = item - before;
-      const bool first = k < na;
-      // fetch the owner's triangle (both candidates, then select)
-      Tri<D> t;
+      if (mine.nrows > 0) {
+        DepositMaps M = mine.map == 0 ? m_total : (mine.map == 1 ? m_min : m_sad);
+        deposit_row<D>(mine, mine.rlo, npx, M);
+      }
+      const int extra = mine.nrows > 1 ? mine.nrows - 1 : 0;
+      int incl = extra;
 #pragma unroll
-      for (int q = 0; q < 3; q++) {
-        D xa_ = __shfl_sync(0xffffffffu, ta.x[q], owner), xb_ = __shfl_sync(0xffffffffu, tb.x[q], owner);
-        D ya_ = __shfl_sync(0xffffffffu, ta.y[q], owner), yb_ = __shfl_sync(0xffffffffu, tb.y[q], owner);
-        D ia_ = __shfl_sync(0xffffffffu, ta.idx[q], owner), ib_ = __shfl_sync(0xffffffffu, tb.idx[q], owner);
-        D ja_ = __shfl_sync(0xffffffffu, ta.idy[q], owner), jb_ = __shfl_sync(0xffffffffu, tb.idy[q], owner);
-        t.x[q] = first ? xa_ : xb_;
-        t.y[q] = first ? ya_ : yb_;
-        t.idx[q] = first ? ia_ : ib_;
-        t.idy[q] = first ? ja_ : jb_;
+      for (int o = 1; o < 32; o <<= 1) {
+        int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
       }
-      {
-        D sa = __shfl_sync(0xffffffffu, ta.scale, owner), sb = __shfl_sync(0xffffffffu, tb.scale, owner);
-        int oxa = __shfl_sync(0xffffffffu, ta.ox, owner), oxb = __shfl_sync(0xffffffffu, tb.ox, owner);
-        int oya = __shfl_sync(0xffffffffu, ta.oy, owner), oyb = __shfl_sync(0xffffffffu, tb.oy, owner);
-        int rla = __shfl_sync(0xffffffffu, ta.rlo, owner), rlb = __shfl_sync(0xffffffffu, tb.rlo, owner);
-        int mpa = __shfl_sync(0xffffffffu, ta.map, owner), mpb = __shfl_sync(0xffffffffu, tb.map, owner);
-        t.scale = first ? sa : sb;
-        t.ox = first ? oxa : oxb;
-        t.oy = first ? oya : oyb;
-        t.rlo = first ? rla : rlb;
-        t.map = first ? mpa : mpb;
-      }
-      if (item < total) {
-        const int r = t.rlo + (first ? k : k - na);
-        DepositMaps M = t.map == 0 ? m_total : (t.map == 1 ? m_min : m_sad);
-        deposit_row<D>(t, r, npx, M);
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      for (int it0 = 0; it0 < total; it0 += 32) {
+        const int item = it0 + lane;
+        int lo = 0, hi = 31;  // owner: first lane whose inclusive count exceeds item
+#pragma unroll
+        for (int step = 0; step < 5; step++) {
+          int mid = (lo + hi) >> 1;
+          int v = __shfl_sync(0xffffffffu, incl, mid);
+          if (v > item) hi = mid;
+          else lo = mid + 1;
+        }
+        const int owner = lo;
+        const int before = __shfl_sync(0xffffffffu, incl - extra, owner);
+        Tri<D> t;
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+          t.x[q] = __shfl_sync(0xffffffffu, mine.x[q], owner);
+          t.y[q] = __shfl_sync(0xffffffffu, mine.y[q], owner);
+          t.sl[q] = __shfl_sync(0xffffffffu, mine.sl[q], owner);
+          t.idy[q] = __shfl_sync(0xffffffffu, mine.idy[q], owner);
+        }
+        t.scale = __shfl_sync(0xffffffffu, mine.scale, owner);
+        t.ox = __shfl_sync(0xffffffffu, mine.ox, owner);
+        t.oy = __shfl_sync(0xffffffffu, mine.oy, owner);
+        t.rlo = __shfl_sync(0xffffffffu, mine.rlo, owner);
+        t.map = __shfl_sync(0xffffffffu, mine.map, owner);
+        if (item < total) {
+          DepositMaps M = t.map == 0 ? m_total : (t.map == 1 ? m_min : m_sad);
+          deposit_row<D>(t, t.rlo + 1 + (item - before), npx, M);
+        }
       }
     }
   }

@@ -479,6 +479,7 @@ class MapMaker {
     lp.coef32 = leaves_.coef32.p;
     lp.rect = tiles_.rect.p;
     lp.tile_off = tiles_.tile_off.p;
+    lp.table = tiles_.table.p;
     lp.nleaves = leaves_.n;
     return lp;
   }

@@ -12,7 +12,8 @@
 //        c_l = (sum_k b_k C(l+k-1,k-1)/(-dz)^k - b_0/l) / dz^l       fmm.cuh:281-322
 //   P2L  dz = (z_i - c_to)/hl_to,
 //        c_0 = sum m_i (log(-dz) + log(hl_to)), c_l = -sum m_i/(l dz^l) fmm.cuh:387-413
-// evaluated with the reference's Horner ordering. Level schedule as
+// evaluated with the reference's Horner ordering, dividing by dz through one
+// reciprocal per interaction (FP64 throughout). Level schedule as
 // include/ipm.cuh:874-901: P2M+M2M bottom-up, then L2L, M2L, P2L top-down from
 // level 2. The reference builds an int binomial table, which overflows beyond
 // order ~17 (binomial_coefficients.cuh:11-44); this table is int64, exact up to
@@ -95,10 +96,11 @@ __global__ void fmm_m2m(int beg, int end, int p, const T* __restrict__ cx, const
       } else {
         double hc = hl[c];
         cplx<double> dz = mk((double(cx[c]) - double(cx[k])) / hc, (double(cy[c]) - double(cy[k])) / hc);
+        const cplx<double> idz = cdiv(mk(1.0, 0.0), dz);
         r = mk(0.0, 0.0);
         for (int i = p; i >= 1; i--) {
           r = cadd(r, cscale(ld2(a + i), binom(btab, lane - 1, i - 1)));
-          r = cdiv(r, dz);
+          r = cmul(r, idz);
         }
         r = csub(r, cdivr(ld2(a), double(lane)));
         r = cmul(r, cpowi(dz, lane));
@@ -146,11 +148,12 @@ __global__ void fmm_local(int beg, int end, int p, const T* __restrict__ cx, con
       double hf = hl[f];
       cplx<double> d = mk((double(cx[f]) - ccx) / hf, (double(cy[f]) - ccy) / hf);
       cplx<double> md = cneg(d);
+      const cplx<double> imd = cdiv(mk(1.0, 0.0), md);
       cplx<double> t = mk(0.0, 0.0);
       if (lane == 0) {
         for (int i = p; i >= 1; i--) {
           t = cadd(t, ld2(b + i));
-          t = cdiv(t, md);
+          t = cmul(t, imd);
         }
         cplx<double> b0 = ld2(b);
         t = cadd(t, cmul(b0, clog_(md)));
@@ -158,10 +161,10 @@ __global__ void fmm_local(int beg, int end, int p, const T* __restrict__ cx, con
       } else {
         for (int i = p; i >= 1; i--) {
           t = cadd(t, cscale(ld2(b + i), binom(btab, lane + i - 1, i - 1)));
-          t = cdiv(t, md);
+          t = cmul(t, imd);
         }
         t = csub(t, cdivr(ld2(b), double(lane)));
-        t = cdiv(t, cpowi(d, lane));
+        t = cmul(t, cpowi(cneg(imd), lane));  // 1 / d^l
       }
       acc = cadd(acc, t);
     }
@@ -179,7 +182,8 @@ __global__ void fmm_local(int beg, int end, int p, const T* __restrict__ cx, con
           t = cadd(t, cscale(clog_(cneg(d)), m));
           t.re += m * log(h);
         } else {
-          t = csub(t, cdiv(mk(m, 0.0), cscale(cpowi(d, lane), double(lane))));
+          // m / (l d^l) = (m / l) (1/d)^l
+          t = csub(t, cscale(cpowi(cdiv(mk(1.0, 0.0), d), lane), m / double(lane)));
         }
       }
       acc = cadd(acc, t);

@@ -47,9 +47,28 @@ struct LatticeTiles {
   DevVec<int4> rect;  // i0, i1, j0, j1
   DevVec<long long> tiles;
   DevVec<long long> tile_off;  // [n + 1]
+  DevVec<int4> table;          // per tile: leaf, i0, j0, (ni << 16) | nj
   long long total = 0;
   ScanScratch scan;
 };
+
+// One thread per leaf writes the table entries of its tiles (row-major over
+// the leaf's rectangle).
+__global__ void leaf_tile_table(int nleaves, const int4* __restrict__ rect, const long long* __restrict__ tile_off,
+                                int tx, int ty, int4* __restrict__ table) {
+  for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < nleaves; l += gridDim.x * blockDim.x) {
+    int4 r = rect[l];
+    long long t = tile_off[l], t_end = tile_off[l + 1];
+    if (t == t_end) continue;
+    int ntx = (r.y - r.x + tx - 1) / tx;
+    for (long long k = 0; t + k < t_end; k++) {
+      int tj = int(k / ntx), ti = int(k % ntx);
+      int i0 = r.x + ti * tx, j0 = r.z + tj * ty;
+      int ni = min(tx, r.y - i0), nj = min(ty, r.w - j0);
+      table[t + k] = make_int4(l, i0, j0, (ni << 16) | nj);
+    }
+  }
+}
 
 __global__ void leaf_flags(int n, const int* __restrict__ child0, int* flag) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) flag[k] = child0[k] < 0;
@@ -204,6 +223,9 @@ bool build_lattice_tiles(LatticeTiles& W, const LeafSet& L, TreeDev<T>& t, doubl
   IRSB_CKR(cudaMemcpyAsync(W.tile_off.p + L.n, W.scan.sum.p, sizeof(long long), cudaMemcpyDeviceToDevice, s));
   IRSB_CKR(cudaMemcpyAsync(&W.total, W.scan.sum.p, sizeof(long long), cudaMemcpyDeviceToHost, s));
   IRSB_CKR(cudaStreamSynchronize(s));
+  if (!W.table.alloc_exact(std::max<long long>(W.total, 1))) return false;
+  leaf_tile_table<<<blocks, 256, 0, s>>>(L.n, W.rect.p, W.tile_off.p, kTileX, kTileY, W.table.p);
+  IRSB_LAUNCH_CK("leaf_tile_table");
   return true;
 }
 

@@ -64,6 +64,7 @@ struct LeafPtrs {
   const float2* coef32;
   const int4* rect;
   const long long* tile_off;
+  const int4* table;  // per tile: leaf, i0, j0, (ni << 16) | nj
   int nleaves;
 };
 
@@ -84,16 +85,13 @@ struct TileInfo {
 };
 
 __device__ __forceinline__ TileInfo tile_info(const LeafPtrs& lp, long long t) {
+  int4 e = lp.table[t];
   TileInfo ti;
-  ti.leaf = find_leaf(lp.tile_off, lp.nleaves, t);
-  int4 r = lp.rect[ti.leaf];
-  long long local = t - lp.tile_off[ti.leaf];
-  int ntx = (r.y - r.x + kTileX - 1) / kTileX;
-  int tj = int(local / ntx), tix = int(local % ntx);
-  ti.i0 = r.x + tix * kTileX;
-  ti.j0 = r.z + tj * kTileY;
-  ti.ni = min(kTileX, r.y - ti.i0);
-  ti.nj = min(kTileY, r.w - ti.j0);
+  ti.leaf = e.x;
+  ti.i0 = e.y;
+  ti.j0 = e.z;
+  ti.ni = e.w >> 16;
+  ti.nj = e.w & 0xffff;
   return ti;
 }
 
@@ -301,32 +299,40 @@ __global__ void __launch_bounds__(kShootThreads) shoot_f32(ShootParams sp, LeafP
           sy[r] = s;
         }
       }
-      // ---- far field + output
+      // ---- far field: Horner in dz = u / hl, one coefficient read per 4 points
+      float Ar[R], Ai[R], Dr[R], Di[R], dzr[R], dzi[R];
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        dzr[r] = ux * inv_hl;
+        dzi[r] = uy[r] * inv_hl;
+        Ar[r] = Ai[r] = Dr[r] = Di[r] = 0.f;
+      }
+      for (int k = sp.p - 1; k >= 0; k--) {
+        const float2 c = s_coef[k];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          if (PAR && k >= 1) {  // derivative polynomial sum k e_k dz^(k-1)
+            float tr = fmaf(Dr[r], dzr[r], -Di[r] * dzi[r]);
+            float tt = fmaf(Dr[r], dzi[r], Di[r] * dzr[r]);
+            Dr[r] = fmaf(c.x, float(k), tr);
+            Di[r] = fmaf(c.y, float(k), tt);
+          }
+          float tr = fmaf(Ar[r], dzr[r], -Ai[r] * dzi[r]);
+          float tt = fmaf(Ar[r], dzi[r], Ai[r] * dzr[r]);
+          Ar[r] = tr + c.x;
+          Ai[r] = tt + c.y;
+        }
+      }
+      // ---- output
 #pragma unroll
       for (int r = 0; r < R; r++) {
         const int jj = ty + r * RS;
         if (jj >= ti.nj) break;
         const long long j = ti.j0 + jj;
-        const float dzr = ux * inv_hl, dzi = uy[r] * inv_hl;
-        float Ar = 0.f, Ai = 0.f, Dr = 0.f, Di = 0.f;
-        for (int k = sp.p - 1; k >= 0; k--) {
-          if (PAR && k >= 1) {  // derivative polynomial sum k e_k dz^(k-1)
-            float tr = fmaf(Dr, dzr, -Di * dzi);
-            float tt = fmaf(Dr, dzi, Di * dzr);
-            float2 c = s_coef[k];
-            Dr = fmaf(c.x, float(k), tr);
-            Di = fmaf(c.y, float(k), tt);
-          }
-          float tr = fmaf(Ar, dzr, -Ai * dzi);
-          float tt = fmaf(Ar, dzi, Ai * dzr);
-          float2 c = s_coef[k];
-          Ar = tr + c.x;
-          Ai = tt + c.y;
-        }
         const float Sx = sx[r] + cxr[r], Sy = sy[r] + cyr[r];
         // w - w(centre) = lin * u - alpha_star - conj(A)
-        const float wr = fmaf(flin_x, ux, -(Sx + Ar));
-        const float wi = fmaf(flin_y, uy[r], -(Sy - Ai));
+        const float wr = fmaf(flin_x, ux, -(Sx + Ar[r]));
+        const float wi = fmaf(flin_y, uy[r], -(Sy - Ai[r]));
         double px = pcx + double(wr) * scx;
         double py = pcy + double(wi) * scy;
         if (GENERIC_SMOOTH) {
@@ -350,7 +356,7 @@ __global__ void __launch_bounds__(kShootThreads) shoot_f32(ShootParams sp, LeafP
             // d alpha_star / d zbar = -conj(sum m theta^2 / d^2) ; sum m/d^2 = sum q conj(d)^2/|d|^2
             double dsr = -double(dxx[r]), dsi = -double(dxy[r]);
             // d alpha_local / d zbar = conj(A'(dz)) / hl
-            double dlr = double(Dr) * double(inv_hl), dli = -double(Di) * double(inv_hl);
+            double dlr = double(Dr[r]) * double(inv_hl), dli = -double(Di[r]) * double(inv_hl);
             double dwdz = (1.0 - sp.kappa) - dsz;
             double gr = sp.gamma - dsr - dlr - dszb.re, gi = -dsi - dli - dszb.im;
             double mu = 1.0 / (dwdz * dwdz - (gr * gr + gi * gi));

@@ -29,6 +29,7 @@
  * structure in a reproducible order.
  */
 #define _GNU_SOURCE
+#include <float.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -974,22 +975,27 @@ void orc_ipm_deposit_ref(long long ncx, long long ncy, const double* vx, const d
 #define CAT(a, b) CAT2(a, b)
 #define FN(name) CAT(name, SUF)
 #define TRI(suf) CAT(Tri, suf)
+#define STRIP(suf) CAT(Strip, suf)
 
 #define D float
 #define SUF f32
 #define RINT llrintf
+#define DMAX FLT_MAX
 #include "fixdep.inc"
 #undef D
 #undef SUF
 #undef RINT
+#undef DMAX
 
 #define D double
 #define SUF f64
 #define RINT llrint
+#define DMAX DBL_MAX
 #include "fixdep.inc"
 #undef D
 #undef SUF
 #undef RINT
+#undef DMAX
 
 /* ------------------------------------------------------------ derived parameters (double) */
 /* calculate_derived_params, include/ipm.cuh:434-506 for a generated circular or

@@ -107,6 +107,17 @@ def test_fixed_point_conserves_area():
     assert abs(q.sum() - 2 * 20 * 26) < 1e-6
 
 
+@pytest.mark.parametrize("step", [1.0, 0.5, 2.0])
+@pytest.mark.parametrize("single", [False, True])
+def test_fixed_point_pixel_aligned_cells(step, single):
+    # cell edges exactly on pixel lines (no deflection): an edge on the line
+    # between two rows must be counted once
+    v = np.stack(np.meshgrid(np.arange(5, 26, step), np.arange(4, 31, step)), -1)
+    q = po.ipm_deposit_fixed(v, 1.0, (40, 40), single=single).astype(np.float64) / 2.0 ** 32
+    ref = po.ipm_deposit_ref(v, 1.0, (40, 40))
+    np.testing.assert_array_equal(q, ref)
+
+
 @pytest.mark.parametrize("order,tol", [(8, 5e-3), (16, 5e-6), (24, 5e-9)])
 def test_expansion_converges_to_direct_sum(order, tol):
     rng = np.random.default_rng(0)
