@@ -240,6 +240,49 @@ def reference_arm(args):
     print(json.dumps(out))
 
 
+def batch_measure(steps):
+    """The batched form: 256 realizations of uneven size (1024^2 maps, half
+    length 12) through the graph-captured pipeline, timed per replay; then the
+    plain uniform FP64 form of every realization run singly at the same
+    expansion order, timed by its device pipeline, and the FP32 batch maps'
+    error against those FP64 maps."""
+    import irs_b200
+    from irs_b200.batch import random_realizations
+
+    reals, redrawn = random_realizations()
+    b = irs_b200.BatchIPM(reals)
+    t0 = time.perf_counter()
+    b.run()
+    first = time.perf_counter() - t0
+    ts = [b.rerun(1) for _ in range(max(2, steps))]
+    t_batch = float(np.mean(ts))
+    pix, cells = b.value("total_pixels"), b.value("total_cells")
+    order = int(b.value("expansion_order"))
+    maps = b.maps
+    res = {"realizations": len(reals), "redrawn": redrawn, "stars": int(b.value("total_stars")), "cells": int(cells),
+           "pixels": int(pix), "order": order, "passes": int(b.value("passes")),
+           "graph_nodes": int(b.value("graph_nodes")), "graph_replay_ms": t_batch * 1e3,
+           "pixels_per_s": pix / t_batch, "cells_per_s": cells / t_batch, "first_run_s": first,
+           "stars_and_moments_ms": b.value("t_stars") * 1e3}
+    b.close()
+    t_plain, med, mx = 0.0, [], []
+    for r, kw in enumerate(reals):
+        s = irs_b200.IPM(**kw, is_double=True, expansion_order=order)
+        s.run()
+        t_plain += s.rerun(1)
+        ref = s.magnifications
+        s.close()
+        ok = ref > 0
+        rel = np.abs(maps[r][ok].astype(np.float64) - ref[ok]) / ref[ok]
+        med.append(float(np.median(rel)))
+        mx.append(float(rel.max()))
+    res.update({"plain_fp64_s": t_plain, "plain_fp64_pixels_per_s": pix / t_plain,
+                "batched_fp32_over_plain_fp64": t_plain / t_batch,
+                "median_rel_err_vs_fp64": {"median_of_maps": float(np.median(med)), "max_of_maps": float(np.max(med))},
+                "max_rel_err_vs_fp64": float(np.max(mx))})
+    return res
+
+
 def our_arm(args):
     import torch
 
@@ -358,6 +401,7 @@ def our_arm(args):
                           "ms_per_step": float(np.mean(ts)) * 1e3, "shoot_ms": r.value("t_lattice") * 1e3,
                           "rays_received": int(r.num_rays_received)}
             r.close()
+        extra["batched_256"] = batch_measure(args.steps)
 
     if rank == 0:
         cpu = cpu_baseline(m, stars.astype(np.float64), os.cpu_count() or 1) if (ws == 1 and not args.no_cpu) else None

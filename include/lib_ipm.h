@@ -136,6 +136,27 @@ bool copy_fixed_maps(IPMHandle* self, unsigned long long* total, unsigned long l
 int ipm_deposit_noalloc(const double* verts, long long ncx, long long ncy, IPM_DTYPE factor, int npx, int npy,
                         IPM_DTYPE* map, void* stream);
 
+/* Batches of realizations (no counterpart in the reference): many star
+ * fields (own seed, convergence, shear, smooth fraction, mass function; one
+ * map size) through one device pipeline whose tree build, expansions,
+ * shooting and deposition are captured in one CUDA graph and replayed.
+ * Realizations are described by objects of this library (init + setters) and
+ * copied in by batch_add. The FP32 form is used; each map equals a single
+ * run of the same inputs at the same expansion order (set_precision(2) on a
+ * double object). */
+void* batch_init(void);
+void batch_destroy(void* batch);
+int batch_add(void* batch, IPMHandle* realization);   /* returns its index */
+int batch_size(void* batch);
+void batch_set_expansion_order(void* batch, int order);     /* 0: largest reference-formula order */
+void batch_set_corner_capacity(void* batch, long long n);   /* corner positions per pass; 0: automatic */
+bool batch_run(void* batch, int verbose);
+bool batch_rerun(void* batch, int repeats, double* seconds); /* replay on the resident star fields */
+bool batch_copy_maps(void* batch, IPM_DTYPE* out);           /* [size][npy][npx] */
+const IPM_DTYPE* batch_maps_device(void* batch);             /* the same maps on the device */
+bool batch_copy_stars(void* batch, IPM_DTYPE* out);          /* all star fields, tree order, (x1, x2, m) */
+double batch_get_value(void* batch, int r, const char* name); /* r >= 0: realization value; r < 0: batch value */
+
 #ifdef __cplusplus
 }
 #endif

@@ -4,6 +4,8 @@ The compute path is hand-written CUDA for sm_100a behind a C ABI
 (include/lib_ipm.h, include/lib_irs.h); this package holds the ctypes
 interface. Build the libraries with `python -m irs_b200.build`.
 """
+from .adaptive import AdaptiveIPM, LevelNet  # noqa: F401
+from .batch import BatchIPM  # noqa: F401
 from .mapmaker import IPM, IRS  # noqa: F401
 
-__all__ = ["IPM", "IRS"]
+__all__ = ["IPM", "IRS", "BatchIPM", "AdaptiveIPM", "LevelNet"]

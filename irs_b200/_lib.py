@@ -44,6 +44,13 @@ EXTENSION_SYMBOLS = [
     "copy_coeffs", "get_num_vertices", "copy_vertices", "copy_fixed_maps",
 ]
 IRS_ONLY_SYMBOLS = ["get_t_shoot_rays", "get_num_rays_shot", "get_num_rays_received"]
+IPM_ONLY_SYMBOLS = ["ipm_deposit_noalloc", "batch_init", "batch_destroy", "batch_add", "batch_size",
+                    "batch_set_expansion_order", "batch_set_corner_capacity", "batch_run", "batch_rerun",
+                    "batch_copy_maps", "batch_maps_device", "batch_copy_stars", "batch_get_value",
+                    "ada_init", "ada_destroy", "ada_base", "ada_set_policy", "ada_set_levels", "ada_set_tolerance",
+                    "ada_set_audit", "ada_set_refine_capacity", "ada_set_network", "ada_run", "ada_num_tiles",
+                    "ada_copy_features", "ada_copy_levels", "ada_labels", "ada_copy_map", "ada_get_value",
+                    "mlp_num_params", "mlp_train", "mlp_gradients", "mlp_predict"]
 
 LIB_NAMES = {
     ("ipm", False): "lib_ipm.so",
@@ -142,6 +149,47 @@ def _bind(lib, kind: str, is_double: bool):
     lib.copy_vertices.restype = C.c_bool
     lib.copy_fixed_maps.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.copy_fixed_maps.restype = C.c_bool
+    if kind == "ipm":
+        lib.batch_init.argtypes = []
+        lib.batch_init.restype = vp
+        lib.batch_destroy.argtypes = [vp]
+        lib.batch_destroy.restype = None
+        lib.batch_add.argtypes = [vp, vp]
+        lib.batch_add.restype = C.c_int
+        lib.batch_size.argtypes = [vp]
+        lib.batch_size.restype = C.c_int
+        lib.batch_set_expansion_order.argtypes = [vp, C.c_int]
+        lib.batch_set_expansion_order.restype = None
+        lib.batch_set_corner_capacity.argtypes = [vp, C.c_longlong]
+        lib.batch_set_corner_capacity.restype = None
+        lib.batch_run.argtypes = [vp, C.c_int]
+        lib.batch_run.restype = C.c_bool
+        lib.batch_rerun.argtypes = [vp, C.c_int, C.POINTER(C.c_double)]
+        lib.batch_rerun.restype = C.c_bool
+        lib.batch_copy_maps.argtypes = [vp, C.c_void_p]
+        lib.batch_copy_maps.restype = C.c_bool
+        lib.batch_maps_device.argtypes = [vp]
+        lib.batch_maps_device.restype = C.c_void_p
+        lib.batch_copy_stars.argtypes = [vp, C.c_void_p]
+        lib.batch_copy_stars.restype = C.c_bool
+        lib.batch_get_value.argtypes = [vp, C.c_int, C.c_char_p]
+        lib.batch_get_value.restype = C.c_double
+        fp, ip = C.c_void_p, C.c_void_p
+        for name, args, res in [
+                ("ada_init", [], vp), ("ada_destroy", [vp], None), ("ada_base", [vp], vp),
+                ("ada_set_policy", [vp, C.c_int, C.c_int], None), ("ada_set_levels", [vp, ip, C.c_int], None),
+                ("ada_set_tolerance", [vp, C.c_double], None), ("ada_set_audit", [vp, C.c_double, C.c_uint], None),
+                ("ada_set_refine_capacity", [vp, C.c_longlong], None), ("ada_set_network", [vp, fp, fp, fp], None),
+                ("ada_run", [vp, C.c_int], C.c_bool), ("ada_num_tiles", [vp], C.c_int),
+                ("ada_copy_features", [vp, fp], C.c_bool), ("ada_copy_levels", [vp, ip, C.c_int], C.c_bool),
+                ("ada_labels", [vp, ip, C.c_int, ip, fp], C.c_bool), ("ada_copy_map", [vp, C.c_void_p], C.c_bool),
+                ("ada_get_value", [vp, C.c_char_p], C.c_double), ("mlp_num_params", [], C.c_int),
+                ("mlp_train", [fp, ip, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint, fp, fp, fp, fp], C.c_bool),
+                ("mlp_gradients", [fp, fp, fp, fp, ip, C.c_int, fp, fp], C.c_bool),
+                ("mlp_predict", [fp, fp, fp, fp, C.c_int, ip], C.c_bool)]:
+            f = getattr(lib, name)
+            f.argtypes = args
+            f.restype = res
     return lib
 
 

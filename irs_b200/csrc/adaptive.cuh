@@ -1,0 +1,377 @@
+// Adaptive IPM: per-tile subdivision of the lens-plane cell lattice.
+//
+// The cell lattice of a map (num_rays_y cells per unlensed pixel area) is cut
+// into tiles of kAdaTile x kAdaTile cells. A tile at level s (1, 2, 4, 8, 16)
+// splits each of its cells into s x s subcells: its corner lattice has
+// kAdaTile * s + 1 points per side at spacing 2 * rhs / s, and each subcell
+// deposits factor / s^2 through the same fixed-point deposition as the
+// uniform lattice. Level 16 everywhere is the uniform-fine map; level 1
+// everywhere is the plain map.
+//
+// Corner positions of a refined tile:
+//   * points of the base lattice are taken from the base corner buffer (the
+//     tiled lens-equation pass), so tiles of every level share them exactly;
+//   * points on an edge shared with a coarser neighbour (level s' < s) are
+//     placed on the straight segment between that neighbour's corners, so the
+//     refined lattice is conforming (no gaps or overlaps between tiles);
+//   * other points are evaluated one by one: descent of the quadtree to the
+//     leaf that owns the point (the boxes that partition the lattice for the
+//     tiled pass), then the FP32 leaf-relative lens equation of shoot_f32
+//     (compensated near-field sum, FP32 Horner of FP64-built coefficients,
+//     FP64 conversion to pixels). A point's position depends only on its
+//     global fine index, so neighbouring tiles compute shared points
+//     identically.
+//
+// Labels for training: a tile's label is the smallest level s whose
+// piecewise-linear interpolation over its cells' two triangles (the shape the
+// deposition gives each triangle) misplaces at most a share eps of the
+// tile's flux against the level-16 positions (ada_level_errors; 16 when no
+// coarser level does).
+#pragma once
+#include "deposit.cuh"
+#include "leaves.cuh"
+#include "shoot.cuh"
+#include "tree.cuh"
+
+namespace irsb {
+
+constexpr int kAdaTile = 32;         // cells per tile side
+constexpr int kAdaMaxLevel = 16;     // finest subdivision
+constexpr int kAdaLevels = 5;        // 1, 2, 4, 8, 16
+constexpr int kAdaFeatures = 8;
+
+__host__ __device__ __forceinline__ int ada_level_of(int cls) { return 1 << cls; }
+__host__ __device__ __forceinline__ long long llmin_(long long a, long long b) { return a < b ? a : b; }
+
+// Tree nodes needed by the descent, and the node -> leaf map.
+template <typename T>
+struct DescentPtrs {
+  const T* cx;
+  const T* cy;
+  const int* child0;
+  const long long* leaf_of_node;  // exclusive scan of the leaf flags
+};
+
+template <typename T>
+__device__ __forceinline__ int descend_leaf(const DescentPtrs<T>& d, double x, double y) {
+  int k = 0;
+  for (int it = 0; it < kMaxLevels + 1; it++) {
+    const int c0 = d.child0[k];
+    if (c0 < 0) break;
+    const double cx = double(d.cx[k]), cy = double(d.cy[k]);
+    const bool right = x >= cx, top = y >= cy;
+    k = c0 + (right ? (top ? 0 : 3) : (top ? 1 : 2));
+  }
+  return int(d.leaf_of_node[k]);
+}
+
+// Source position (pixel units, row axis flipped) of the lattice point (x, y)
+// evaluated with leaf `leaf`: the arithmetic of shoot_f32 for one point, so a
+// base lattice point gets the same position from either kernel.
+template <bool GENERIC_SMOOTH>
+__device__ __forceinline__ double2 eval_point_f32(const ShootParams& sp, const LeafPtrs& lp, int leaf, double x,
+                                                  double y) {
+  const double lcx = lp.cx[leaf], lcy = lp.cy[leaf];
+  const float inv_hl = float(1.0 / lp.hl[leaf]);
+  const double lin_x = 1.0 - sp.kappa + sp.kstar + sp.gamma;
+  const double lin_y = 1.0 - sp.kappa + sp.kstar - sp.gamma;
+  const double scx = sp.npx / (2.0 * sp.hly_re), scy = sp.npy / (2.0 * sp.hly_im);
+  const double pcx = ((lin_x * lcx - sp.cy_re) + sp.hly_re) * scx;
+  const double pcy = ((lin_y * lcy - sp.cy_im) + sp.hly_im) * scy;
+  const float ux = float(x - lcx), uy = float(y - lcy);
+  const int nn = lp.nnear[leaf];
+  const float4* near = lp.near32 + (size_t)leaf * kMaxStarsDirect;
+  float sx = 0.f, sy = 0.f, cxr = 0.f, cyr = 0.f;
+  for (int s0 = 0; s0 < nn; s0 += 4) {
+    float bx = 0.f, by = 0.f;
+    for (int s = s0; s < s0 + 4 && s < nn; s++) {
+      const float4 st = near[s];
+      const float ex = ux - st.x, ey = uy - st.y;
+      const float r2 = fmaf(ex, ex, ey * ey);
+      const float q = st.z * rcp_approx(r2);
+      bx = fmaf(q, ex, bx);
+      by = fmaf(q, ey, by);
+    }
+    float t = sx + bx, bb = t - sx;
+    cxr += (sx - (t - bb)) + (bx - bb);
+    sx = t;
+    t = sy + by;
+    bb = t - sy;
+    cyr += (sy - (t - bb)) + (by - bb);
+    sy = t;
+  }
+  const float2* coef = lp.coef32 + (size_t)leaf * kMaxOrder;
+  const float dzr = ux * inv_hl, dzi = uy * inv_hl;
+  float Ar = 0.f, Ai = 0.f;
+  for (int k = sp.p - 1; k >= 0; k--) {
+    const float2 c = coef[k];
+    const float tr = fmaf(Ar, dzr, -Ai * dzi);
+    const float tt = fmaf(Ar, dzi, Ai * dzr);
+    Ar = tr + c.x;
+    Ai = tt + c.y;
+  }
+  const float Sx = sx + cxr, Sy = sy + cyr;
+  const float wr = fmaf(float(lin_x), ux, -(Sx + Ar));
+  const float wi = fmaf(float(lin_y), uy, -(Sy - Ai));
+  double px = pcx + double(wr) * scx;
+  double py = pcy + double(wi) * scy;
+  if (GENERIC_SMOOTH) {
+    const cplx<double> corner = mk(sp.corner_re, sp.corner_im);
+    const cplx<double> z = mk(lcx + double(ux), lcy + double(uy));
+    const cplx<double> a_sm = alpha_smooth_(z, sp.kstar, sp.rect, corner, sp.approx, sp.taylor_smooth, sp.inv_pi);
+    px += (-a_sm.re - sp.kstar * z.re) * scx;
+    py += (-a_sm.im - sp.kstar * z.im) * scy;
+  }
+  return make_double2(px, double(sp.npy) - py);
+}
+
+// Lattice coordinate of global fine index F (16 fine steps per base cell):
+// base points (F multiple of 16) reproduce the base lattice formula exactly.
+__device__ __forceinline__ double fine_coord(double base, double rhs, long long F) {
+  return base + 2.0 * (rhs * (double(F) * (1.0 / kAdaMaxLevel)));
+}
+
+// Geometry of the adaptive pass of one map.
+struct AdaGeom {
+  double base_x, base_y, rhs_x, rhs_y;  // corner lattice (cell corners)
+  long long ncx, ncy;                   // cells of the base lattice
+  int ntx, nty;                         // tiles
+  int npx, npy;                         // map
+};
+
+// A source position (pixels) that can reach the map: inside it or within
+// kAdaMargin pixels of its border.
+constexpr double kAdaMargin = 2.0;
+__device__ __forceinline__ bool ada_on_map(const AdaGeom& g, double2 p) {
+  return p.x >= -kAdaMargin && p.x <= g.npx + kAdaMargin && p.y >= -kAdaMargin && p.y <= g.npy + kAdaMargin;
+}
+
+// Corner (a, b) of tile t at level s, in the tile's corner grid
+// [0, ncell_x * s] x [0, ncell_y * s].
+template <typename T, bool GENERIC_SMOOTH>
+__device__ __forceinline__ double2 tile_corner(const AdaGeom& g, const ShootParams& sp, const LeafPtrs& lp,
+                                               const DescentPtrs<T>& dp, const double2* __restrict__ base_verts,
+                                               int tx, int ty, int s, int a, int b) {
+  const long long i0 = (long long)tx * kAdaTile, j0 = (long long)ty * kAdaTile;
+  if (a % s == 0 && b % s == 0) {
+    const long long i = i0 + a / s, j = j0 + b / s;
+    return base_verts[j * (g.ncx + 1) + i];
+  }
+  const long long F = (i0 * kAdaMaxLevel) + (long long)a * (kAdaMaxLevel / s);
+  const long long G = (j0 * kAdaMaxLevel) + (long long)b * (kAdaMaxLevel / s);
+  const double x = fine_coord(g.base_x, g.rhs_x, F), y = fine_coord(g.base_y, g.rhs_y, G);
+  return eval_point_f32<GENERIC_SMOOTH>(sp, lp, descend_leaf(dp, x, y), x, y);
+}
+
+// Refined corner grids of the tiles in `list` (all at level s), written at
+// out + slot * stride with row stride ncell_x * s + 1. One thread per corner.
+// Points on an edge shared with a coarser neighbour (tile_level, per tile) are
+// placed on that neighbour's edge segment; without tile_level every point is
+// evaluated.
+template <typename T, bool GENERIC_SMOOTH>
+__global__ void __launch_bounds__(256) ada_refine_corners(AdaGeom g, ShootParams sp, LeafPtrs lp, DescentPtrs<T> dp,
+                                                          const double2* __restrict__ base_verts,
+                                                          const int* __restrict__ tile_level,
+                                                          const int* __restrict__ list, int nlist, int s,
+                                                          long long stride, double2* __restrict__ out) {
+  const int side = kAdaTile * s + 1;
+  const long long per_tile = (long long)side * side;
+  const long long total = per_tile * nlist;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int slot = int(q / per_tile);
+    const int rem = int(q - (long long)slot * per_tile);
+    int b = rem / side, a = rem - b * side;
+    const int t = list[slot];
+    const int tx = t % g.ntx, ty = t / g.ntx;
+    const int ncx_t = int(llmin_(kAdaTile, g.ncx - (long long)tx * kAdaTile));
+    const int ncy_t = int(llmin_(kAdaTile, g.ncy - (long long)ty * kAdaTile));
+    const int wa = ncx_t * s, hb = ncy_t * s;  // corner grid extent of this (possibly partial) tile
+    if (a > wa || b > hb) continue;
+    // neighbour across the edge this point lies on (a point on two edges is a
+    // tile corner, hence a base point)
+    int nlev = s;
+    bool along_b = false;  // the edge runs along b (left / right edge)
+    if (!tile_level) {
+      // isolated tiles (labels, audit): every point evaluated
+    } else if (a == 0 && tx > 0) {
+      nlev = tile_level[t - 1];
+      along_b = true;
+    } else if (a == wa && tx + 1 < g.ntx && wa == kAdaTile * s) {
+      nlev = tile_level[t + 1];
+      along_b = true;
+    } else if (b == 0 && ty > 0) {
+      nlev = tile_level[t - g.ntx];
+    } else if (b == hb && ty + 1 < g.nty && hb == kAdaTile * s) {
+      nlev = tile_level[t + g.ntx];
+    }
+    double2 p;
+    if (nlev < s && !(a % s == 0 && b % s == 0)) {
+      const int step = s / nlev;
+      const int u = along_b ? b : a;
+      const int u0 = (u / step) * step, u1 = u0 + step;
+      const double2 p0 = along_b ? tile_corner<T, GENERIC_SMOOTH>(g, sp, lp, dp, base_verts, tx, ty, s, a, u0)
+                                 : tile_corner<T, GENERIC_SMOOTH>(g, sp, lp, dp, base_verts, tx, ty, s, u0, b);
+      const double2 p1 = along_b ? tile_corner<T, GENERIC_SMOOTH>(g, sp, lp, dp, base_verts, tx, ty, s, a, u1)
+                                 : tile_corner<T, GENERIC_SMOOTH>(g, sp, lp, dp, base_verts, tx, ty, s, u1, b);
+      const double f = double(u - u0) / double(step);
+      p = make_double2(p0.x + (p1.x - p0.x) * f, p0.y + (p1.y - p0.y) * f);
+    } else {
+      p = tile_corner<T, GENERIC_SMOOTH>(g, sp, lp, dp, base_verts, tx, ty, s, a, b);
+    }
+    out[(long long)slot * stride + (long long)b * (wa + 1) + a] = p;
+  }
+}
+
+// Interpolation error of levels 1, 2, 4, 8 against the level-16 corner grid
+// of each tile in `list` (grid at fine + slot * stride, row stride
+// ncell_x * 16 + 1), as the share of deposited flux that the coarser level
+// misplaces: at every fine corner where either position can reach the map,
+// the distance (pixels) between the level-16 position and the piecewise-linear
+// interpolation of level 2^c over the two triangles of the level-2^c cell
+// containing it, divided by that cell's image size (its longest edge, at
+// least one pixel: a displacement moves about distance / size of an image
+// larger than a pixel across pixel borders, and about the distance itself of
+// a smaller one). err[slot * 4 + c] is the mean over those corners; every
+// cell carries the same flux, so the mean weights them equally. Near a star
+// the lens map runs off with diverging curvature, but its images there are
+// stretched, so the relative measure keeps those corners in proportion.
+// One block per tile.
+__global__ void __launch_bounds__(256) ada_level_errors(AdaGeom g, const int* __restrict__ list, int nlist,
+                                                        long long stride, const double2* __restrict__ fine,
+                                                        float* __restrict__ err) {
+  __shared__ double red_s[4][8];
+  __shared__ int red_n[4][8];
+  for (int slot = blockIdx.x; slot < nlist; slot += gridDim.x) {
+    const int t = list[slot];
+    const int tx = t % g.ntx, ty = t / g.ntx;
+    const int ncx_t = int(llmin_(kAdaTile, g.ncx - (long long)tx * kAdaTile));
+    const int ncy_t = int(llmin_(kAdaTile, g.ncy - (long long)ty * kAdaTile));
+    const int W = ncx_t * kAdaMaxLevel + 1, H = ncy_t * kAdaMaxLevel + 1;
+    const double2* P = fine + (long long)slot * stride;
+    double sum[4] = {0, 0, 0, 0};
+    int cnt[4] = {0, 0, 0, 0};
+    for (int q = threadIdx.x; q < W * H; q += blockDim.x) {
+      const int b = q / W, a = q - b * W;
+      const double2 v = P[q];
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const int step = kAdaMaxLevel >> c;  // fine corners per level-2^c cell side
+        int a0 = (a / step) * step, b0 = (b / step) * step;
+        if (a0 == W - 1) a0 -= step;
+        if (b0 == H - 1) b0 -= step;
+        const double u = double(a - a0) / step, w = double(b - b0) / step;
+        // cell corners: y2 = (a0, b0), y3 = (a1, b0), y0 = (a1, b1), y1 = (a0, b1);
+        // triangles (y0, y1, y2) for u <= w and (y2, y3, y0) for u >= w
+        const double2 p2 = P[(long long)b0 * W + a0], p0 = P[(long long)(b0 + step) * W + a0 + step];
+        const double2 p1 = P[(long long)(b0 + step) * W + a0], p3 = P[(long long)b0 * W + a0 + step];
+        double2 r;
+        if (u <= w)
+          r = make_double2(p2.x + w * (p1.x - p2.x) + u * (p0.x - p1.x), p2.y + w * (p1.y - p2.y) + u * (p0.y - p1.y));
+        else
+          r = make_double2(p2.x + u * (p3.x - p2.x) + w * (p0.x - p3.x), p2.y + u * (p3.y - p2.y) + w * (p0.y - p3.y));
+        if (ada_on_map(g, v) || ada_on_map(g, r)) {
+          const double size = fmax(fmax(hypot(p3.x - p2.x, p3.y - p2.y), hypot(p1.x - p2.x, p1.y - p2.y)),
+                                   fmax(hypot(p0.x - p1.x, p0.y - p1.y), hypot(p0.x - p3.x, p0.y - p3.y)));
+          const double e = hypot(r.x - v.x, r.y - v.y) / fmax(size, 1.0);
+          if (!isnan(e)) {
+            sum[c] += e;
+            cnt[c]++;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      double v = sum[c];
+      int k = cnt[c];
+      for (int o = 16; o > 0; o >>= 1) {
+        v += __shfl_down_sync(0xffffffffu, v, o);
+        k += __shfl_down_sync(0xffffffffu, k, o);
+      }
+      if ((threadIdx.x & 31) == 0) {
+        red_s[c][threadIdx.x >> 5] = v;
+        red_n[c][threadIdx.x >> 5] = k;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+      double v = 0;
+      long long k = 0;
+      for (int w = 0; w < int(blockDim.x >> 5); w++) {
+        v += red_s[threadIdx.x][w];
+        k += red_n[threadIdx.x][w];
+      }
+      err[(long long)slot * 4 + threadIdx.x] = k ? float(v / double(k)) : 0.f;
+    }
+    __syncthreads();
+  }
+}
+
+// Per-tile features from the base corner lattice and the tree (one thread per
+// tile):
+//   0  smooth convergence kappa_tot - kappa_star
+//   1  star convergence kappa_star
+//   2  mean shear magnitude of the local Jacobian at the tile's 4 corner cells
+//   3  log10 of the smallest |det J| at those cells (J = d source / d lens, in
+//      pixels per unlensed pixel, from the cell's edge vectors)
+//   4  log10 of the largest |det J|
+//   5  1 when det J changes sign between those cells (a critical curve runs
+//      through the tile), else 0
+//   6  log10 of the distance from the tile centre to the nearest star of the
+//      leaf that owns the centre (its near field), in cell widths
+//   7  log10 of the largest image edge length (pixels) of those cells
+template <typename T>
+__global__ void ada_features(AdaGeom g, ShootParams sp, LeafPtrs lp, DescentPtrs<T> dp,
+                             const double2* __restrict__ base_verts, float* __restrict__ feat) {
+  const int ntiles = g.ntx * g.nty;
+  const double cellpx = 2.0 * sp.rhs_x * sp.npx / (2.0 * sp.hly_re);  // unlensed cell width in pixels
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
+    const int tx = t % g.ntx, ty = t / g.ntx;
+    const long long i0 = (long long)tx * kAdaTile, j0 = (long long)ty * kAdaTile;
+    const long long ilast = llmin_(i0 + kAdaTile, g.ncx) - 1, jlast = llmin_(j0 + kAdaTile, g.ncy) - 1;
+    const long long ci[4] = {i0, ilast, i0, ilast}, cj[4] = {j0, j0, jlast, jlast};
+    double gsum = 0, dmin = 1e300, dmax = 0, emax = 0;
+    int npos = 0, nneg = 0;
+    for (int k = 0; k < 4; k++) {
+      const long long i = ci[k], j = cj[k], vx = g.ncx + 1;
+      const double2 p00 = base_verts[j * vx + i], p10 = base_verts[j * vx + i + 1],
+                    p01 = base_verts[(j + 1) * vx + i];
+      // d(source)/d(lens) per unlensed pixel; the stored row axis is flipped
+      const double a = (p10.x - p00.x) / cellpx, c = -(p10.y - p00.y) / cellpx;
+      const double b = (p01.x - p00.x) / cellpx, d = -(p01.y - p00.y) / cellpx;
+      const double det = a * d - b * c;
+      const double g1 = 0.5 * (a - d), g2 = 0.5 * (b + c);
+      gsum += sqrt(g1 * g1 + g2 * g2);
+      const double ad = fabs(det);
+      dmin = fmin(dmin, ad);
+      dmax = fmax(dmax, ad);
+      if (det >= 0) npos++;
+      else nneg++;
+      emax = fmax(emax, fmax(hypot(p10.x - p00.x, p10.y - p00.y), hypot(p01.x - p00.x, p01.y - p00.y)));
+    }
+    // nearest star of the near field at the tile centre
+    const double xc = g.base_x + 2.0 * (g.rhs_x * (double(i0) + 0.5 * double(ilast - i0 + 1)));
+    const double yc = g.base_y + 2.0 * (g.rhs_y * (double(j0) + 0.5 * double(jlast - j0 + 1)));
+    const int leaf = descend_leaf(dp, xc, yc);
+    const int nn = lp.nnear[leaf];
+    double dn = 1e300;
+    const double lcx = lp.cx[leaf], lcy = lp.cy[leaf];
+    for (int s = 0; s < nn; s++) {
+      const float4 st = lp.near32[(size_t)leaf * kMaxStarsDirect + s];
+      dn = fmin(dn, hypot(xc - (lcx + double(st.x)), yc - (lcy + double(st.y))));
+    }
+    if (nn == 0) dn = 2.0 * lp.hl[leaf];
+    float* f = feat + (long long)t * kAdaFeatures;
+    f[0] = float(sp.kappa - sp.kstar);
+    f[1] = float(sp.kstar);
+    f[2] = float(gsum * 0.25);
+    f[3] = float(log10(dmin + 1e-6));
+    f[4] = float(log10(dmax + 1e-6));
+    f[5] = (npos > 0 && nneg > 0) ? 1.f : 0.f;
+    f[6] = float(log10(dn / (2.0 * sp.rhs_x) + 1e-6));
+    f[7] = float(log10(emax + 1e-6));
+  }
+}
+
+}  // namespace irsb

@@ -8,6 +8,8 @@
 // (microlensing/IPM/lib_ipm.py) binds them unchanged. The IRS libraries use
 // the same conventions (the reference has no IRS library). Declarations and
 // the list of extensions are in include/lib_ipm.h and include/lib_irs.h.
+#include "adaptive_host.cuh"
+#include "batch.cuh"
 #include "engine.cuh"
 
 #include <cstring>
@@ -302,6 +304,141 @@ int ipm_deposit_noalloc(const double* verts, long long ncx, long long ncy, dtype
   irsb::ipm_finalize<dtype><<<g2, 256, 0, s>>>(npix, m.acc, nullptr, nullptr, map, nullptr, nullptr, 0);
   if (cudaGetLastError() != cudaSuccess) return 4;
   return 0;
+}
+
+// ---------------------------------------------------------------- batches
+// Many realizations through one graph-captured device pipeline (no
+// counterpart in the reference). A realization is described by an object of
+// this library (init + setters) and copied into the batch by batch_add.
+using Batch = irsb::BatchMaker<dtype>;
+
+void* batch_init() { return new Batch(); }
+void batch_destroy(void* b) { delete static_cast<Batch*>(b); }
+int batch_add(void* b, Obj* realization) {
+  Batch* bt = static_cast<Batch*>(b);
+  bt->in.push_back(realization->prm);
+  return bt->size() - 1;
+}
+int batch_size(void* b) { return static_cast<Batch*>(b)->size(); }
+void batch_set_expansion_order(void* b, int p) { static_cast<Batch*>(b)->expansion_order = p; }
+void batch_set_corner_capacity(void* b, long long n) { static_cast<Batch*>(b)->corner_cap = n; }
+bool batch_run(void* b, int verbose) { return static_cast<Batch*>(b)->run(verbose); }
+bool batch_rerun(void* b, int repeats, double* seconds) { return static_cast<Batch*>(b)->rerun(repeats, seconds); }
+bool batch_copy_maps(void* b, dtype* out) { return static_cast<Batch*>(b)->copy_maps(out); }
+const dtype* batch_maps_device(void* b) { return static_cast<Batch*>(b)->maps_device(); }
+bool batch_copy_stars(void* b, dtype* out) { return static_cast<Batch*>(b)->copy_stars(out); }
+// r >= 0: a realization's derived value; r < 0: a value of the batch
+double batch_get_value(void* b, int r, const char* name) {
+  Batch* bt = static_cast<Batch*>(b);
+  std::string n = name ? name : "";
+  if (r < 0) {
+    if (n == "size") return bt->size();
+    if (n == "expansion_order") return bt->order;
+    if (n == "passes") return bt->passes;
+    if (n == "total_cells") return double(bt->total_cells);
+    if (n == "total_pixels") return double(bt->total_pixels);
+    if (n == "total_stars") return double(bt->total_stars);
+    if (n == "t_stars") return bt->t_stars;
+    if (n == "t_graph") return bt->t_graph;
+    if (n == "graph_nodes") return bt->graph_nodes;
+    if (n == "num_pixels_y1") return bt->npx();
+    if (n == "num_pixels_y2") return bt->npy();
+    return std::numeric_limits<double>::quiet_NaN();
+  }
+  if (r >= int(bt->prm.size())) return std::numeric_limits<double>::quiet_NaN();
+  const auto& p = bt->prm[r];
+  if (n == "num_stars") return p.num_stars;
+  if (n == "star_offset") return double(bt->star_offset(r));
+  if (n == "num_cells") return double(p.num_ray_threads.re) * p.num_ray_threads.im;
+  if (n == "tree_levels") return p.tree_levels;
+  if (n == "expansion_order") return p.expansion_order;
+  if (n == "mu_ave") return p.mu_ave;
+  if (n == "kappa_tot") return p.kappa_tot;
+  if (n == "shear") return p.shear;
+  if (n == "kappa_star") return p.kappa_star;
+  if (n == "corner_x1") return p.corner.re;
+  if (n == "corner_x2") return p.corner.im;
+  if (n == "root_half_length") return p.root_half_length;
+  if (n == "mean_mass_actual") return p.mean_mass_actual;
+  if (n == "kappa_star_actual") return p.kappa_star_actual;
+  if (n == "random_seed") return p.random_seed;
+  return std::numeric_limits<double>::quiet_NaN();
+}
+
+// ---------------------------------------------------------------- adaptive IPM
+// Per-tile subdivision chosen by the level network (no counterpart in the
+// reference). The map inputs are set on the object returned by ada_base with
+// the setters of this library.
+using Ada = irsb::AdaptiveIPM<dtype>;
+
+void* ada_init() { return new Ada(); }
+void ada_destroy(void* a) { delete static_cast<Ada*>(a); }
+Obj* ada_base(void* a) { return &static_cast<Ada*>(a)->base; }
+void ada_set_policy(void* a, int policy, int uniform_level) {
+  static_cast<Ada*>(a)->policy = policy;
+  static_cast<Ada*>(a)->uniform_level = uniform_level;
+}
+void ada_set_levels(void* a, const int* levels, int n) {
+  static_cast<Ada*>(a)->given_levels.assign(levels, levels + n);
+}
+void ada_set_tolerance(void* a, double eps_px) { static_cast<Ada*>(a)->eps = eps_px; }
+void ada_set_audit(void* a, double fraction, unsigned seed) {
+  static_cast<Ada*>(a)->audit_fraction = fraction;
+  static_cast<Ada*>(a)->audit_seed = seed;
+}
+void ada_set_refine_capacity(void* a, long long n) { static_cast<Ada*>(a)->refine_cap = n; }
+void ada_set_network(void* a, const float* w, const float* mu, const float* sig) {
+  Ada* ad = static_cast<Ada*>(a);
+  ad->net_w.assign(w, w + irsb::kMlpParams);
+  ad->net_mu.assign(mu, mu + irsb::kMlpIn);
+  ad->net_sig.assign(sig, sig + irsb::kMlpIn);
+}
+bool ada_run(void* a, int verbose) { return static_cast<Ada*>(a)->run(verbose); }
+int ada_num_tiles(void* a) { return static_cast<Ada*>(a)->num_tiles(); }
+bool ada_copy_features(void* a, float* out) { return static_cast<Ada*>(a)->copy_features(out); }
+bool ada_copy_levels(void* a, int* out, int predicted) {
+  Ada* ad = static_cast<Ada*>(a);
+  const std::vector<int>& v = predicted ? ad->predicted : ad->level;
+  std::copy(v.begin(), v.end(), out);
+  return true;
+}
+bool ada_labels(void* a, const int* tiles, int n, int* labels, float* err) {
+  std::vector<int> t(tiles, tiles + n), lab;
+  std::vector<float> e;
+  if (!static_cast<Ada*>(a)->labels(t, lab, e)) return false;
+  std::copy(lab.begin(), lab.end(), labels);
+  if (err) std::copy(e.begin(), e.end(), err);
+  return true;
+}
+bool ada_copy_map(void* a, dtype* out) { return static_cast<Ada*>(a)->copy_map(out); }
+double ada_get_value(void* a, const char* name) {
+  Ada* ad = static_cast<Ada*>(a);
+  std::string n = name ? name : "";
+  if (n == "tiles_x") return ad->ntx;
+  if (n == "tiles_y") return ad->nty;
+  if (n == "cells_base") return double(ad->cells_base);
+  if (n == "cells_evaluated") return double(ad->cells_evaluated);
+  if (n == "audit_cells") return double(ad->audit_cells);
+  if (n == "audited") return ad->audited;
+  if (n == "audit_failures") return ad->audit_failures;
+  if (n == "t_base") return ad->t_base;
+  if (n == "t_adapt") return ad->t_adapt;
+  if (n == "tolerance") return ad->eps;
+  return get_value(&ad->base, name);
+}
+
+// The level network on its own: training, gradients and prediction.
+int mlp_num_params() { return irsb::kMlpParams; }
+bool mlp_train(const float* feat, const int* labels, int n, int epochs, int batch, float lr, unsigned seed, float* w,
+               float* mu, float* sig, float* epoch_loss) {
+  return irsb::MlpTrainer::train(feat, labels, n, epochs, batch, lr, seed, w, mu, sig, epoch_loss);
+}
+bool mlp_gradients(const float* w, const float* mu, const float* sig, const float* feat, const int* labels, int n,
+                   float* grad, float* mean_loss) {
+  return irsb::MlpTrainer::gradients(w, mu, sig, feat, labels, n, grad, mean_loss);
+}
+bool mlp_predict(const float* w, const float* mu, const float* sig, const float* feat, int n, int* cls) {
+  return irsb::MlpTrainer::predict(w, mu, sig, feat, n, cls);
 }
 
 }  // extern "C"

@@ -33,6 +33,9 @@ enum DeviceError : int {
   kErrSameLevelOverflow = 2,
   kErrDiffLevelOverflow = 4,
   kErrNearOverflow = 8,
+  kErrTableOverflow = 16,   // lattice tile table capacity (graph-captured pipelines)
+  kErrNodeOverflow = 32,    // node capacity (graph-captured pipelines)
+  kErrLevelOverflow = 64,   // more tree levels than the captured build holds
 };
 
 #define IRSB_HD __host__ __device__ __forceinline__

@@ -313,77 +313,128 @@ __device__ __forceinline__ void deposit_row(const Tri<D>& t, int r, int npx, Dep
 // finding its item's owner lane by a binary search over the scan and reading
 // the triangle through shuffles, so a triangle with many rows is spread over
 // the warp instead of holding one lane.
+// The 32 cells [base, base + 32) of an ncx-wide lattice whose corner rows are
+// vx apart (whole warp; lanes past ncells idle).
 template <typename D>
-__global__ void __launch_bounds__(256, sizeof(D) == 4 ? 4 : 2) ipm_deposit_cells(const double2* __restrict__ verts, long long ncx,
-                                                            long long ncy, D factor, int npx, int npy,
-                                                            DepositMaps m_total, DepositMaps m_min,
-                                                            DepositMaps m_sad, int parities) {
-  const long long ncells = ncx * ncy;
-  const long long vx = ncx + 1;
+__device__ __forceinline__ void deposit_warp_cells(const double2* __restrict__ verts, long long ncx, long long vx,
+                                                   long long ncells, long long base, D factor, int npx, int npy,
+                                                   const DepositMaps& m_total, const DepositMaps& m_min,
+                                                   const DepositMaps& m_sad, int parities) {
   const int lane = threadIdx.x & 31;
+  const long long c = base + lane;
+  double2 y0 = make_double2(0, 0), y1 = y0, y2 = y0, y3 = y0;
+  if (c < ncells) {
+    long long j = c / ncx, i = c - j * ncx;
+    y0 = verts[(j + 1) * vx + (i + 1)];  // z + rhs
+    y1 = verts[(j + 1) * vx + i];        // z - conj(rhs)
+    y2 = verts[j * vx + i];              // z - rhs
+    y3 = verts[j * vx + (i + 1)];        // z + conj(rhs)
+  }
+#pragma unroll 1
+  for (int half = 0; half < 2; half++) {
+    Tri<D> mine;
+    mine.nrows = 0;
+    if (c < ncells) {
+      mine = half == 0 ? setup_triangle<D>(y0.x, y0.y, y1.x, y1.y, y2.x, y2.y, factor, npx, npy, parities != 0)
+                       : setup_triangle<D>(y2.x, y2.y, y3.x, y3.y, y0.x, y0.y, factor, npx, npy, parities != 0);
+    }
+    if (mine.nrows > 0) {
+      DepositMaps M = mine.map == 0 ? m_total : (mine.map == 1 ? m_min : m_sad);
+      deposit_row<D>(mine, mine.rlo, npx, M);
+    }
+    const int extra = mine.nrows > 1 ? mine.nrows - 1 : 0;
+    int incl = extra;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    for (int it0 = 0; it0 < total; it0 += 32) {
+      const int item = it0 + lane;
+      int lo = 0, hi = 31;  // owner: first lane whose inclusive count exceeds item
+#pragma unroll
+      for (int step = 0; step < 5; step++) {
+        int mid = (lo + hi) >> 1;
+        int v = __shfl_sync(0xffffffffu, incl, mid);
+        if (v > item) hi = mid;
+        else lo = mid + 1;
+      }
+      const int owner = lo;
+      const int before = __shfl_sync(0xffffffffu, incl - extra, owner);
+      Tri<D> t;
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        t.x[q] = __shfl_sync(0xffffffffu, mine.x[q], owner);
+        t.y[q] = __shfl_sync(0xffffffffu, mine.y[q], owner);
+        t.sl[q] = __shfl_sync(0xffffffffu, mine.sl[q], owner);
+        t.idy[q] = __shfl_sync(0xffffffffu, mine.idy[q], owner);
+      }
+      t.scale = __shfl_sync(0xffffffffu, mine.scale, owner);
+      t.ox = __shfl_sync(0xffffffffu, mine.ox, owner);
+      t.oy = __shfl_sync(0xffffffffu, mine.oy, owner);
+      t.rlo = __shfl_sync(0xffffffffu, mine.rlo, owner);
+      t.map = __shfl_sync(0xffffffffu, mine.map, owner);
+      if (item < total) {
+        DepositMaps M = t.map == 0 ? m_total : (t.map == 1 ? m_min : m_sad);
+        deposit_row<D>(t, t.rlo + 1 + (item - before), npx, M);
+      }
+    }
+  }
+}
+
+// Cells of an ncx x ncy lattice whose (ncx+1) x (ncy+1) corner positions are in
+// `verts`. A warp takes 32 consecutive cells and handles their first
+// triangles, then their second triangles: each lane prepares one triangle and
+// deposits its first row; the warp then scans the counts of the remaining
+// rows and works through those (triangle, row) items 32 at a time, each lane
+// finding its item's owner lane by a binary search over the scan and reading
+// the triangle through shuffles, so a triangle with many rows is spread over
+// the warp instead of holding one lane.
+template <typename D>
+__global__ void __launch_bounds__(256, sizeof(D) == 4 ? 4 : 2)
+    ipm_deposit_cells(const double2* __restrict__ verts, long long ncx, long long ncy, D factor, int npx, int npy,
+                      DepositMaps m_total, DepositMaps m_min, DepositMaps m_sad, int parities) {
+  const long long ncells = ncx * ncy;
   const long long warp0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  for (long long base = warp0 * 32; base < ncells; base += nwarps * 32) {
-    const long long c = base + lane;
-    double2 y0 = make_double2(0, 0), y1 = y0, y2 = y0, y3 = y0;
-    if (c < ncells) {
-      long long j = c / ncx, i = c - j * ncx;
-      y0 = verts[(j + 1) * vx + (i + 1)];  // z + rhs
-      y1 = verts[(j + 1) * vx + i];        // z - conj(rhs)
-      y2 = verts[j * vx + i];              // z - rhs
-      y3 = verts[j * vx + (i + 1)];        // z + conj(rhs)
+  for (long long base = warp0 * 32; base < ncells; base += nwarps * 32)
+    deposit_warp_cells<D>(verts, ncx, ncx + 1, ncells, base, factor, npx, npy, m_total, m_min, m_sad, parities);
+}
+
+// A block of cells inside a pass of the batched (or adaptive) deposition: its
+// corner rows start at `voff` in the pass's corner buffer, vstride apart.
+template <typename D>
+struct DepositPiece {
+  long long voff;
+  long long vstride;   // corner row stride (ncx + 1 for a whole lattice row)
+  long long ncx, ncy;  // cells
+  long long chunk0;    // first 32-cell chunk of the piece in the pass
+  D factor;
+  int r;               // realization (map index)
+};
+
+// Batched deposition: the warps stride over the 32-cell chunks of all pieces
+// of the pass; a chunk's piece is found by a binary search over chunk0.
+// Realization r accumulates into the maps at r * map_stride / r * diff_stride.
+template <typename D>
+__global__ void __launch_bounds__(256, sizeof(D) == 4 ? 4 : 2)
+    ipm_deposit_batch(const double2* __restrict__ verts, const DepositPiece<D>* __restrict__ pieces, int npieces,
+                      long long nchunks, int npx, int npy, DepositMaps maps, long long map_stride,
+                      long long diff_stride) {
+  const long long warp0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long g = warp0; g < nchunks; g += nwarps) {
+    int lo = 0, hi = npieces - 1;  // last piece with chunk0 <= g
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (pieces[mid].chunk0 <= g) lo = mid;
+      else hi = mid - 1;
     }
-#pragma unroll 1
-    for (int half = 0; half < 2; half++) {
-      Tri<D> mine;
-      mine.nrows = 0;
-      if (c < ncells) {
-        mine = half == 0 ? setup_triangle<D>(y0.x, y0.y, y1.x, y1.y, y2.x, y2.y, factor, npx, npy, parities != 0)
-                         : setup_triangle<D>(y2.x, y2.y, y3.x, y3.y, y0.x, y0.y, factor, npx, npy, parities != 0);
-      }
-      if (mine.nrows > 0) {
-        DepositMaps M = mine.map == 0 ? m_total : (mine.map == 1 ? m_min : m_sad);
-        deposit_row<D>(mine, mine.rlo, npx, M);
-      }
-      const int extra = mine.nrows > 1 ? mine.nrows - 1 : 0;
-      int incl = extra;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-      }
-      const int total = __shfl_sync(0xffffffffu, incl, 31);
-      for (int it0 = 0; it0 < total; it0 += 32) {
-        const int item = it0 + lane;
-        int lo = 0, hi = 31;  // owner: first lane whose inclusive count exceeds item
-#pragma unroll
-        for (int step = 0; step < 5; step++) {
-          int mid = (lo + hi) >> 1;
-          int v = __shfl_sync(0xffffffffu, incl, mid);
-          if (v > item) hi = mid;
-          else lo = mid + 1;
-        }
-        const int owner = lo;
-        const int before = __shfl_sync(0xffffffffu, incl - extra, owner);
-        Tri<D> t;
-#pragma unroll
-        for (int q = 0; q < 3; q++) {
-          t.x[q] = __shfl_sync(0xffffffffu, mine.x[q], owner);
-          t.y[q] = __shfl_sync(0xffffffffu, mine.y[q], owner);
-          t.sl[q] = __shfl_sync(0xffffffffu, mine.sl[q], owner);
-          t.idy[q] = __shfl_sync(0xffffffffu, mine.idy[q], owner);
-        }
-        t.scale = __shfl_sync(0xffffffffu, mine.scale, owner);
-        t.ox = __shfl_sync(0xffffffffu, mine.ox, owner);
-        t.oy = __shfl_sync(0xffffffffu, mine.oy, owner);
-        t.rlo = __shfl_sync(0xffffffffu, mine.rlo, owner);
-        t.map = __shfl_sync(0xffffffffu, mine.map, owner);
-        if (item < total) {
-          DepositMaps M = t.map == 0 ? m_total : (t.map == 1 ? m_min : m_sad);
-          deposit_row<D>(t, t.rlo + 1 + (item - before), npx, M);
-        }
-      }
-    }
+    const DepositPiece<D> pc = pieces[lo];
+    const DepositMaps M{maps.acc + pc.r * map_stride, maps.diff + pc.r * diff_stride};
+    deposit_warp_cells<D>(verts + pc.voff, pc.ncx, pc.vstride, pc.ncx * pc.ncy, (g - pc.chunk0) * 32, pc.factor,
+                          npx, npy, M, M, M, 0);
   }
 }
 

@@ -93,8 +93,10 @@ constexpr int kScanItems = 4;  // per thread
 constexpr int kScanTile = kScanBlock * kScanItems;
 
 template <typename In>
-__global__ void scan_block_totals(const In* __restrict__ in, long long n, long long* __restrict__ totals) {
+__global__ void scan_block_totals(const In* __restrict__ in, long long n, const int* __restrict__ dn,
+                                  long long* __restrict__ totals) {
   __shared__ long long red[kScanBlock / 32];
+  if (dn) n = *dn;
   long long base = (long long)blockIdx.x * kScanTile;
   long long s = 0;
   for (int k = 0; k < kScanItems; k++) {
@@ -147,9 +149,10 @@ __global__ void scan_totals_single(long long* __restrict__ totals, long long m, 
 }
 
 template <typename In>
-__global__ void scan_block_apply(const In* __restrict__ in, long long n, const long long* __restrict__ offsets,
-                                 long long* __restrict__ out) {
+__global__ void scan_block_apply(const In* __restrict__ in, long long n, const int* __restrict__ dn,
+                                 const long long* __restrict__ offsets, long long* __restrict__ out) {
   __shared__ long long warp_sums[kScanBlock / 32];
+  if (dn) n = *dn;
   __shared__ long long carry;
   if (threadIdx.x == 0) carry = offsets[blockIdx.x];
   __syncthreads();
@@ -194,10 +197,29 @@ bool exclusive_scan(const In* in, long long n, long long* out, ScanScratch& sc, 
   if (nb < 1) nb = 1;
   if (!sc.totals.reserve(size_t(nb), s)) return false;
   if (!sc.sum.reserve(1, s)) return false;
-  scan_block_totals<In><<<unsigned(nb), kScanBlock, 0, s>>>(in, n, sc.totals.p);
+  scan_block_totals<In><<<unsigned(nb), kScanBlock, 0, s>>>(in, n, nullptr, sc.totals.p);
   scan_totals_single<<<1, kScanBlock, 0, s>>>(sc.totals.p, nb, sc.sum.p);
-  scan_block_apply<In><<<unsigned(nb), kScanBlock, 0, s>>>(in, n, sc.totals.p, out);
+  scan_block_apply<In><<<unsigned(nb), kScanBlock, 0, s>>>(in, n, nullptr, sc.totals.p, out);
   return IRSB_CK(cudaGetLastError());
+}
+
+// The same with the element count read on the device from *dn (at most
+// n_cap), for work whose size the host does not know (graph-captured
+// pipelines). The scratch must already hold the blocks for n_cap.
+template <typename In>
+bool exclusive_scan_dev(const In* in, const int* dn, long long n_cap, long long* out, ScanScratch& sc,
+                        cudaStream_t s) {
+  long long nb = (n_cap + kScanTile - 1) / kScanTile;
+  if (nb < 1) nb = 1;
+  scan_block_totals<In><<<unsigned(nb), kScanBlock, 0, s>>>(in, n_cap, dn, sc.totals.p);
+  scan_totals_single<<<1, kScanBlock, 0, s>>>(sc.totals.p, nb, sc.sum.p);
+  scan_block_apply<In><<<unsigned(nb), kScanBlock, 0, s>>>(in, n_cap, dn, sc.totals.p, out);
+  return IRSB_CK(cudaGetLastError());
+}
+
+inline bool scan_reserve(ScanScratch& sc, long long n_cap, cudaStream_t s) {
+  long long nb = (n_cap + kScanTile - 1) / kScanTile;
+  return sc.totals.reserve(size_t(nb < 1 ? 1 : nb), s) && sc.sum.reserve(1, s);
 }
 
 template <typename T>

@@ -36,8 +36,63 @@ enum Precision : int {
   kPrecisionFP32 = 2,
 };
 
+// Kernel parameters of the lens-equation pass over the ray lattice (IRS) or
+// the cell-corner lattice (IPM, vertices), the latter held from row jbase on.
+template <typename T>
+ShootParams make_shoot_params(const Params<T>& p, bool vertices, long long jbase) {
+  ShootParams sp;
+  sp.kappa = double(p.kappa_tot);
+  sp.gamma = double(p.shear);
+  sp.kstar = double(p.kappa_star);
+  sp.theta2 = double(p.theta_star) * double(p.theta_star);
+  sp.inv_pi = 0.318309886183790671537767526745028724;
+  sp.rect = p.rectangular;
+  sp.approx = p.approx;
+  sp.taylor_smooth = p.taylor_smooth;
+  sp.p = p.expansion_order;
+  sp.corner_re = double(p.corner.re);
+  sp.corner_im = double(p.corner.im);
+  sp.cy_re = double(p.center_y.re);
+  sp.cy_im = double(p.center_y.im);
+  sp.hly_re = double(p.half_length_y.re);
+  sp.hly_im = double(p.half_length_y.im);
+  sp.npx = p.num_pixels_y.re;
+  sp.npy = p.num_pixels_y.im;
+  sp.rhs_x = double(p.ray_half_sep.re);
+  sp.rhs_y = double(p.ray_half_sep.im);
+  const double ox = double(p.center_x.re) - double(p.half_length_x.re);
+  const double oy = double(p.center_x.im) - double(p.half_length_x.im);
+  sp.jbase = 0;
+  if (vertices) {
+    sp.base_x = ox;
+    sp.base_y = oy;
+    sp.nx = (long long)p.num_ray_threads.re + 1;
+    sp.ny = (long long)p.num_ray_threads.im + 1;
+    sp.jbase = jbase;
+  } else {
+    sp.base_x = ox + sp.rhs_x;
+    sp.base_y = oy + sp.rhs_y;
+    sp.nx = p.num_ray_threads.re;
+    sp.ny = p.num_ray_threads.im;
+  }
+  return sp;
+}
+
+// Image-plane area of one IPM triangle in pixel units (include/ipm.cuh, the
+// factor of ipm_functions.cuh:170), in the arithmetic type of the deposition.
+template <typename T, typename D>
+D ipm_triangle_factor(const Params<T>& p) {
+  return D(2 * p.ray_half_sep.re * p.ray_half_sep.im * p.num_pixels_y.re * p.num_pixels_y.im /
+           (2 * p.half_length_y.re * 2 * p.half_length_y.im));
+}
+
+template <typename T>
+class AdaptiveIPM;
+
 template <typename T, bool IS_IRS>
 class MapMaker {
+  friend class AdaptiveIPM<T>;
+
  public:
   using Pix = typename std::conditional<IS_IRS, int, T>::type;
   Params<T> prm;
@@ -68,6 +123,9 @@ class MapMaker {
   double t_lattice = 0;      // seconds, lens-equation kernel of the last shoot
   double t_deposit = 0;      // seconds, IPM deposition kernel of the last shoot
   long long launches = 0;    // kernels launched by the last run / pipeline call
+  // IPM: stop after the corner lattice (no deposition, no maps); used by the
+  // adaptive deposition, which deposits the lattice itself
+  bool verts_only = false;
 
   MapMaker() {
     if (IS_IRS) {
@@ -150,7 +208,7 @@ class MapMaker {
     // stars in tree order, as the reference leaves them
     IRSB_CKR(cudaMemcpyAsync(stars_out.data(), d_stars_.p, size_t(n) * sizeof(StarRec<T>), cudaMemcpyDeviceToHost,
                              stream_));
-    if (!post(verbose)) return false;
+    if (!verts_only && !post(verbose)) return false;
     IRSB_CKR(cudaStreamSynchronize(stream_));
     if (verbose >= 1) {
       std::cout << (IS_IRS ? "irs" : "ipm") << ": stars " << n << ", tree levels " << prm.tree_levels
@@ -420,43 +478,7 @@ class MapMaker {
   }
 
   ShootParams shoot_params(bool vertices) const {
-    const Params<T>& p = prm;
-    ShootParams sp;
-    sp.kappa = double(p.kappa_tot);
-    sp.gamma = double(p.shear);
-    sp.kstar = double(p.kappa_star);
-    sp.theta2 = double(p.theta_star) * double(p.theta_star);
-    sp.inv_pi = 0.318309886183790671537767526745028724;
-    sp.rect = p.rectangular;
-    sp.approx = p.approx;
-    sp.taylor_smooth = p.taylor_smooth;
-    sp.p = p.expansion_order;
-    sp.corner_re = double(p.corner.re);
-    sp.corner_im = double(p.corner.im);
-    sp.cy_re = double(p.center_y.re);
-    sp.cy_im = double(p.center_y.im);
-    sp.hly_re = double(p.half_length_y.re);
-    sp.hly_im = double(p.half_length_y.im);
-    sp.npx = p.num_pixels_y.re;
-    sp.npy = p.num_pixels_y.im;
-    sp.rhs_x = double(p.ray_half_sep.re);
-    sp.rhs_y = double(p.ray_half_sep.im);
-    double ox = double(p.center_x.re) - double(p.half_length_x.re);
-    double oy = double(p.center_x.im) - double(p.half_length_x.im);
-    sp.jbase = 0;
-    if (vertices) {
-      sp.base_x = ox;
-      sp.base_y = oy;
-      sp.nx = (long long)p.num_ray_threads.re + 1;
-      sp.ny = (long long)p.num_ray_threads.im + 1;
-      sp.jbase = band_rows().first;
-    } else {
-      sp.base_x = ox + sp.rhs_x;
-      sp.base_y = oy + sp.rhs_y;
-      sp.nx = p.num_ray_threads.re;
-      sp.ny = p.num_ray_threads.im;
-    }
-    return sp;
+    return make_shoot_params(prm, vertices, vertices ? band_rows().first : 0);
   }
 
   // [first, last) lattice rows of this object's band (rays or cells).
@@ -569,17 +591,19 @@ class MapMaker {
       }
       DepositMaps mt{d_acc_.p, d_diff_.p}, mmin{d_acc_min_.p, d_diff_min_.p}, msad{d_acc_sad_.p, d_diff_sad_.p};
       if (!launch_shoot<true>(sp, nullptr, nullptr, nullptr, d_verts_.p)) return false;
+      if (verts_only) {  // the corner lattice is the product (adaptive deposition)
+        IRSB_CKR(cudaEventRecord(ev_dep1_, stream_));
+        return true;
+      }
       const long long ncx = p.num_ray_threads.re, ncy = band.second - band.first;
       long long ncells = ncx * ncy;
       int grid = int(std::max<long long>(1, std::min<long long>((ncells + 255) / 256, 148LL * 16)));
       if (use_fp32()) {
-        float factor = float(2 * p.ray_half_sep.re * p.ray_half_sep.im * p.num_pixels_y.re * p.num_pixels_y.im /
-                             (2 * p.half_length_y.re * 2 * p.half_length_y.im));
+        const float factor = ipm_triangle_factor<T, float>(p);
         ipm_deposit_cells<float><<<grid, 256, 0, stream_>>>(d_verts_.p, ncx, ncy, factor, p.num_pixels_y.re,
                                                             p.num_pixels_y.im, mt, mmin, msad, par ? 1 : 0);
       } else {
-        double factor = double(2 * p.ray_half_sep.re * p.ray_half_sep.im * p.num_pixels_y.re * p.num_pixels_y.im /
-                               (2 * p.half_length_y.re * 2 * p.half_length_y.im));
+        const double factor = ipm_triangle_factor<T, double>(p);
         ipm_deposit_cells<double><<<grid, 256, 0, stream_>>>(d_verts_.p, ncx, ncy, factor, p.num_pixels_y.re,
                                                              p.num_pixels_y.im, mt, mmin, msad, par ? 1 : 0);
       }

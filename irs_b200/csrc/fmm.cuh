@@ -51,9 +51,10 @@ __device__ __forceinline__ double binom(const double* tab, int n, int k) {
 }
 
 template <typename T>
-__global__ void fmm_p2m(int beg, int end, int p, const T* __restrict__ cx, const T* __restrict__ cy,
+__global__ void fmm_p2m(int beg, int end, LevelRange lr, int p, const T* __restrict__ cx, const T* __restrict__ cy,
                         const T* __restrict__ hl, const int* __restrict__ child0, const int* __restrict__ sbeg,
                         const int* __restrict__ scnt, const StarRec<T>* __restrict__ stars, double2* mult) {
+  lr.get(beg, end);
   int lane = threadIdx.x & 31;
   int warps = (gridDim.x * blockDim.x) >> 5;
   for (int k = beg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < end; k += warps) {
@@ -78,9 +79,10 @@ __global__ void fmm_p2m(int beg, int end, int p, const T* __restrict__ cx, const
 
 // Parent multipoles from its 4 children (internal nodes of one level).
 template <typename T>
-__global__ void fmm_m2m(int beg, int end, int p, const T* __restrict__ cx, const T* __restrict__ cy,
+__global__ void fmm_m2m(int beg, int end, LevelRange lr, int p, const T* __restrict__ cx, const T* __restrict__ cy,
                         const T* __restrict__ hl, const int* __restrict__ child0, const double* __restrict__ btab,
                         double2* mult) {
+  lr.get(beg, end);
   int lane = threadIdx.x & 31;
   int warps = (gridDim.x * blockDim.x) >> 5;
   for (int k = beg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < end; k += warps) {
@@ -116,12 +118,13 @@ __global__ void fmm_m2m(int beg, int end, int p, const T* __restrict__ cx, const
 // then M2L over the same-level interaction list, then P2L over the
 // different-level list, accumulated in that order.
 template <typename T>
-__global__ void fmm_local(int beg, int end, int p, const T* __restrict__ cx, const T* __restrict__ cy,
+__global__ void fmm_local(int beg, int end, LevelRange lr, int p, const T* __restrict__ cx, const T* __restrict__ cy,
                           const T* __restrict__ hl, const int* __restrict__ parent, const int* __restrict__ sbeg,
                           const int* __restrict__ scnt, const int* __restrict__ sil, const int* __restrict__ n_sil,
                           const int* __restrict__ dil, const int* __restrict__ n_dil,
                           const StarRec<T>* __restrict__ stars, const double* __restrict__ btab,
                           const double2* __restrict__ mult, double2* loc) {
+  lr.get(beg, end);
   int lane = threadIdx.x & 31;
   int warps = (gridDim.x * blockDim.x) >> 5;
   for (int k = beg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < end; k += warps) {
@@ -212,17 +215,17 @@ bool compute_fmm(FmmDev& f, TreeDev<T>& t, const StarRec<T>* stars, int p, cudaS
     int beg = t.level_off[l], end = t.level_off[l + 1];
     int nw = end - beg;
     int blocks = std::max(1, std::min(ceil_div(nw, 8), 148 * 16));
-    fmm_p2m<T><<<blocks, 256, 0, s>>>(beg, end, p, t.cx.p, t.cy.p, t.hl.p, t.child0.p, t.sbeg.p, t.scnt.p, stars,
+    fmm_p2m<T><<<blocks, 256, 0, s>>>(beg, end, LevelRange{}, p, t.cx.p, t.cy.p, t.hl.p, t.child0.p, t.sbeg.p, t.scnt.p, stars,
                                       f.mult.p);
     IRSB_LAUNCH_CK("fmm_p2m");
-    fmm_m2m<T><<<blocks, 256, 0, s>>>(beg, end, p, t.cx.p, t.cy.p, t.hl.p, t.child0.p, f.btab.p, f.mult.p);
+    fmm_m2m<T><<<blocks, 256, 0, s>>>(beg, end, LevelRange{}, p, t.cx.p, t.cy.p, t.hl.p, t.child0.p, f.btab.p, f.mult.p);
     IRSB_LAUNCH_CK("fmm_m2m");
   }
   for (int l = 2; l <= t.levels; l++) {
     int beg = t.level_off[l], end = t.level_off[l + 1];
     int nw = end - beg;
     int blocks = std::max(1, std::min(ceil_div(nw, 8), 148 * 16));
-    fmm_local<T><<<blocks, 256, 0, s>>>(beg, end, p, t.cx.p, t.cy.p, t.hl.p, t.parent.p, t.sbeg.p, t.scnt.p,
+    fmm_local<T><<<blocks, 256, 0, s>>>(beg, end, LevelRange{}, p, t.cx.p, t.cy.p, t.hl.p, t.parent.p, t.sbeg.p, t.scnt.p,
                                         t.sil.p, t.n_sil.p, t.dil.p, t.n_dil.p, stars, f.btab.p, f.mult.p, f.loc.p);
     IRSB_LAUNCH_CK("fmm_local");
   }

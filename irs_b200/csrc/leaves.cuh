@@ -54,12 +54,18 @@ struct LatticeTiles {
 
 // One thread per leaf writes the table entries of its tiles (row-major over
 // the leaf's rectangle).
-__global__ void leaf_tile_table(int nleaves, const int4* __restrict__ rect, const long long* __restrict__ tile_off,
-                                int tx, int ty, int4* __restrict__ table) {
+__global__ void leaf_tile_table(int nleaves, const int* __restrict__ dn, const int4* __restrict__ rect,
+                                const long long* __restrict__ tile_off, int tx, int ty, int4* __restrict__ table,
+                                long long table_cap, int* __restrict__ err) {
+  if (dn) nleaves = *dn;
   for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < nleaves; l += gridDim.x * blockDim.x) {
     int4 r = rect[l];
     long long t = tile_off[l], t_end = tile_off[l + 1];
     if (t == t_end) continue;
+    if (t_end > table_cap) {  // more tiles than the table holds
+      atomicOr(err, kErrTableOverflow);
+      continue;
+    }
     int ntx = (r.y - r.x + tx - 1) / tx;
     for (long long k = 0; t + k < t_end; k++) {
       int tj = int(k / ntx), ti = int(k % ntx);
@@ -70,32 +76,41 @@ __global__ void leaf_tile_table(int nleaves, const int4* __restrict__ rect, cons
   }
 }
 
-__global__ void leaf_flags(int n, const int* __restrict__ child0, int* flag) {
+__global__ void leaf_flags(int n, const int* __restrict__ dn, const int* __restrict__ child0, int* flag) {
+  if (dn) n = *dn;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) flag[k] = child0[k] < 0;
 }
-__global__ void leaf_compact(int n, const int* __restrict__ flag, const long long* __restrict__ pos, int* node) {
+__global__ void leaf_compact(int n, const int* __restrict__ dn, const int* __restrict__ flag,
+                             const long long* __restrict__ pos, int* node) {
+  if (dn) n = *dn;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
     if (flag[k]) node[pos[k]] = k;
 }
 
 // One warp per leaf: gather the near field and the expansion coefficients.
 template <typename T>
-__global__ void leaf_build(int nleaves, int p, double theta, const int* __restrict__ leaf_node,
+__global__ void leaf_build(int nleaves, const int* __restrict__ dn, int p, double theta,
+                           const double* __restrict__ theta_r, const int* __restrict__ rid,
+                           const int* __restrict__ leaf_node,
                            const T* __restrict__ cx, const T* __restrict__ cy, const T* __restrict__ hl,
                            const int* __restrict__ sbeg, const int* __restrict__ scnt, const int* __restrict__ nbr,
                            const int* __restrict__ n_nbr, const StarRec<T>* __restrict__ stars,
                            const double2* __restrict__ loc, double* lcx, double* lcy, double* lhl, int* nnear,
-                           double4* near64, float4* near32, double2* coef64, float2* coef32, int* dstat) {
+                           double4* near64, float4* near32, double2* coef64, float2* coef32, int* leaf_rid,
+                           int* dstat) {
+  if (dn) nleaves = *dn;
   int lane = threadIdx.x & 31;
   int warps = (gridDim.x * blockDim.x) >> 5;
-  double th2 = theta * theta;
   for (int l = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; l < nleaves; l += warps) {
     int k = leaf_node[l];
+    const double th = theta_r ? theta_r[rid[k]] : theta;
+    const double th2 = th * th;
     double ccx = double(cx[k]), ccy = double(cy[k]), h = double(hl[k]);
     if (lane == 0) {
       lcx[l] = ccx;
       lcy[l] = ccy;
       lhl[l] = h;
+      if (leaf_rid) leaf_rid[l] = rid[k];
     }
     // near list: neighbours in order, then the leaf itself
     int nn = n_nbr[k];
@@ -107,7 +122,8 @@ __global__ void leaf_build(int nleaves, int p, double theta, const int* __restri
         int slot = out + i;
         if (slot < kMaxStarsDirect) {
           StarRec<T> s = stars[b + i];
-          near64[(size_t)l * kMaxStarsDirect + slot] = make_double4(double(s.x), double(s.y), double(s.m), 0.0);
+          if (near64)
+            near64[(size_t)l * kMaxStarsDirect + slot] = make_double4(double(s.x), double(s.y), double(s.m), 0.0);
           near32[(size_t)l * kMaxStarsDirect + slot] =
               make_float4(float(double(s.x) - ccx), float(double(s.y) - ccy), float(double(s.m) * th2), 0.f);
         }
@@ -120,7 +136,7 @@ __global__ void leaf_build(int nleaves, int p, double theta, const int* __restri
     }
     // zero the unused slots so that any over-read is harmless
     for (int slot = out + lane; slot < kMaxStarsDirect; slot += 32) {
-      near64[(size_t)l * kMaxStarsDirect + slot] = make_double4(0, 0, 0, 0);
+      if (near64) near64[(size_t)l * kMaxStarsDirect + slot] = make_double4(0, 0, 0, 0);
       near32[(size_t)l * kMaxStarsDirect + slot] = make_float4(0, 0, 0, 0);
     }
     if (lane == 0) nnear[l] = out;
@@ -128,11 +144,11 @@ __global__ void leaf_build(int nleaves, int p, double theta, const int* __restri
     if (lane < p) {
       int kk = lane + 1;
       double2 c = loc[(size_t)k * (p + 1) + kk];
-      coef64[(size_t)l * kMaxOrder + lane] = make_double2(c.x * kk, c.y * kk);
+      if (coef64) coef64[(size_t)l * kMaxOrder + lane] = make_double2(c.x * kk, c.y * kk);
       double s = th2 * kk / h;
       coef32[(size_t)l * kMaxOrder + lane] = make_float2(float(c.x * s), float(c.y * s));
     } else if (lane < kMaxOrder) {
-      coef64[(size_t)l * kMaxOrder + lane] = make_double2(0, 0);
+      if (coef64) coef64[(size_t)l * kMaxOrder + lane] = make_double2(0, 0);
       coef32[(size_t)l * kMaxOrder + lane] = make_float2(0, 0);
     }
   }
@@ -176,12 +192,51 @@ __global__ void leaf_rects(int nleaves, const int* __restrict__ leaf_node, const
   }
 }
 
+// Lattice of one realization and the rows of it that a pass covers.
+struct LatticeGeom {
+  double base_x, base_y, rhs_x, rhs_y;
+  long long nx, ny;
+};
+
+// leaf_rects over the leaves of many realizations (count on the device): a
+// leaf takes its realization's lattice and that realization's row band
+// [jlo, jhi) of the current pass (empty when jlo >= jhi).
+__global__ void leaf_rects_batch(const int* __restrict__ dn, const int* __restrict__ leaf_node,
+                                 const int* __restrict__ rid, const double* __restrict__ lox,
+                                 const double* __restrict__ hix, const double* __restrict__ loy,
+                                 const double* __restrict__ hiy, const LatticeGeom* __restrict__ geom,
+                                 const long long* __restrict__ jlo_r, const long long* __restrict__ jhi_r, int tx,
+                                 int ty, int4* rect, long long* tiles) {
+  const int nleaves = *dn;
+  for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < nleaves; l += gridDim.x * blockDim.x) {
+    const int k = leaf_node[l];
+    const int r = rid[k];
+    const long long jlo = jlo_r[r], jhi = jhi_r[r];
+    if (jlo >= jhi) {
+      rect[l] = make_int4(0, 0, 0, 0);
+      tiles[l] = 0;
+      continue;
+    }
+    const LatticeGeom g = geom[r];
+    long long i0 = lattice_lower_bound(g.base_x, g.rhs_x, g.nx, lox[k]);
+    long long i1 = lattice_lower_bound(g.base_x, g.rhs_x, g.nx, hix[k]);
+    long long j0 = lattice_lower_bound(g.base_y, g.rhs_y, g.ny, loy[k]);
+    long long j1 = lattice_lower_bound(g.base_y, g.rhs_y, g.ny, hiy[k]);
+    j0 = j0 < jlo ? jlo : j0;
+    j1 = j1 > jhi ? jhi : j1;
+    if (j1 < j0) j1 = j0;
+    rect[l] = make_int4(int(i0), int(i1), int(j0), int(j1));
+    long long ni = i1 - i0, nj = j1 - j0;
+    tiles[l] = (ni > 0 && nj > 0) ? ((ni + tx - 1) / tx) * ((nj + ty - 1) / ty) : 0;
+  }
+}
+
 template <typename T>
 bool build_leaves(LeafSet& L, TreeDev<T>& t, FmmDev& f, const StarRec<T>* stars, double theta, cudaStream_t s) {
   int n = t.num_nodes;
   if (!L.flag.alloc_exact(n) || !L.pos.alloc_exact(n + 1)) return false;
   int blocks = std::max(1, std::min(ceil_div(n, 256), 148 * 8));
-  leaf_flags<<<blocks, 256, 0, s>>>(n, t.child0.p, L.flag.p);
+  leaf_flags<<<blocks, 256, 0, s>>>(n, nullptr, t.child0.p, L.flag.p);
   if (!exclusive_scan<int>(L.flag.p, n, L.pos.p, L.scan, s)) return false;
   long long nl = 0;
   IRSB_CKR(cudaMemcpyAsync(&nl, L.scan.sum.p, sizeof(long long), cudaMemcpyDeviceToHost, s));
@@ -192,13 +247,13 @@ bool build_leaves(LeafSet& L, TreeDev<T>& t, FmmDev& f, const StarRec<T>* stars,
       !L.near32.alloc_exact((size_t)L.n * kMaxStarsDirect) || !L.coef64.alloc_exact((size_t)L.n * kMaxOrder) ||
       !L.coef32.alloc_exact((size_t)L.n * kMaxOrder))
     return false;
-  leaf_compact<<<blocks, 256, 0, s>>>(n, L.flag.p, L.pos.p, L.node.p);
+  leaf_compact<<<blocks, 256, 0, s>>>(n, nullptr, L.flag.p, L.pos.p, L.node.p);
   IRSB_LAUNCH_CK("leaf_compact");
   IRSB_CKR(cudaMemsetAsync(t.dstat.p, 0, 2 * sizeof(int), s));
   int lb = std::max(1, std::min(ceil_div(L.n, 8), 148 * 16));
-  leaf_build<T><<<lb, 256, 0, s>>>(L.n, f.p, theta, L.node.p, t.cx.p, t.cy.p, t.hl.p, t.sbeg.p, t.scnt.p, t.nbr.p,
+  leaf_build<T><<<lb, 256, 0, s>>>(L.n, nullptr, f.p, theta, nullptr, nullptr, L.node.p, t.cx.p, t.cy.p, t.hl.p, t.sbeg.p, t.scnt.p, t.nbr.p,
                                    t.n_nbr.p, stars, f.loc.p, L.cx.p, L.cy.p, L.hl.p, L.nnear.p, L.near64.p,
-                                   L.near32.p, L.coef64.p, L.coef32.p, t.dstat.p);
+                                   L.near32.p, L.coef64.p, L.coef32.p, nullptr, t.dstat.p);
   IRSB_LAUNCH_CK("leaf_build");
   int st = 0;
   IRSB_CKR(cudaMemcpyAsync(&st, t.dstat.p, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -224,7 +279,8 @@ bool build_lattice_tiles(LatticeTiles& W, const LeafSet& L, TreeDev<T>& t, doubl
   IRSB_CKR(cudaMemcpyAsync(&W.total, W.scan.sum.p, sizeof(long long), cudaMemcpyDeviceToHost, s));
   IRSB_CKR(cudaStreamSynchronize(s));
   if (!W.table.alloc_exact(std::max<long long>(W.total, 1))) return false;
-  leaf_tile_table<<<blocks, 256, 0, s>>>(L.n, W.rect.p, W.tile_off.p, kTileX, kTileY, W.table.p);
+  leaf_tile_table<<<blocks, 256, 0, s>>>(L.n, nullptr, W.rect.p, W.tile_off.p, kTileX, kTileY, W.table.p, W.total,
+                                         t.dstat.p + 1);
   IRSB_LAUNCH_CK("leaf_tile_table");
   return true;
 }

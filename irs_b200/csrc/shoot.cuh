@@ -68,20 +68,18 @@ struct LeafPtrs {
   int nleaves;
 };
 
-__device__ __forceinline__ int find_leaf(const long long* __restrict__ off, int n, long long t) {
-  int lo = 0, hi = n;  // off[lo] <= t < off[hi]
-  while (hi - lo > 1) {
-    int mid = (lo + hi) >> 1;
-    if (off[mid] <= t)
-      lo = mid;
-    else
-      hi = mid;
-  }
-  return lo;
-}
-
 struct TileInfo {
   int leaf, i0, j0, ni, nj;
+};
+
+// Destination of a tile's results: IRS maps, or the IPM corner buffer whose
+// row 0 is lattice row vrow0.
+struct ShootOut {
+  int* pix;
+  int* pmin;
+  int* psad;
+  double2* verts;
+  long long vrow0;
 };
 
 __device__ __forceinline__ TileInfo tile_info(const LeafPtrs& lp, long long t) {
@@ -218,13 +216,10 @@ __global__ void __launch_bounds__(kShootThreads) shoot_f64(ShootParams sp, LeafP
 // (alpha_smooth = -kappa_star z); its deviation from that linear form is then
 // added per point in FP64.
 template <bool VERT, bool PAR, bool GENERIC_SMOOTH>
-__global__ void __launch_bounds__(kShootThreads) shoot_f32(ShootParams sp, LeafPtrs lp, long long total_tiles,
-                                                           int* __restrict__ pix, int* __restrict__ pmin,
-                                                           int* __restrict__ psad, double2* __restrict__ verts) {
+__device__ __forceinline__ void shoot_f32_tile(const ShootParams& sp, const LeafPtrs& lp, const TileInfo& ti,
+                                               const ShootOut& o, float4* s_near, float2* s_coef) {
   constexpr int R = kRaysPerThread;
   constexpr int RS = kShootThreads / kTileX;  // row stride between a thread's points
-  __shared__ float4 s_near[kMaxStarsDirect];
-  __shared__ float2 s_coef[kMaxOrder];
   const int tx = threadIdx.x & (kTileX - 1), ty = threadIdx.x / kTileX;
   const cplx<double> corner = mk(sp.corner_re, sp.corner_im);
   // linear part of the lens equation for the circular approximation
@@ -232,9 +227,7 @@ __global__ void __launch_bounds__(kShootThreads) shoot_f32(ShootParams sp, LeafP
   const double lin_y = 1.0 - sp.kappa + sp.kstar - sp.gamma;
   const float flin_x = float(lin_x), flin_y = float(lin_y);
   const double scx = sp.npx / (2.0 * sp.hly_re), scy = sp.npy / (2.0 * sp.hly_im);
-  const float step_y = float(2.0 * sp.rhs_y * RS);
-  for (long long t = blockIdx.x; t < total_tiles; t += gridDim.x) {
-    TileInfo ti = tile_info(lp, t);
+  {
     const int nn = lp.nnear[ti.leaf];
     if (threadIdx.x < kMaxStarsDirect) {
       float4 v = lp.near32[(size_t)ti.leaf * kMaxStarsDirect + threadIdx.x];
@@ -255,11 +248,10 @@ __global__ void __launch_bounds__(kShootThreads) shoot_f32(ShootParams sp, LeafP
       const double xg = sp.base_x + 2.0 * (sp.rhs_x * double(i));
       const float ux = float(xg - lcx);
       const long long j0 = ti.j0 + ty;
-      const double yg0 = sp.base_y + 2.0 * (sp.rhs_y * double(j0));
-      const float uy0 = float(yg0 - lcy);
       float uy[R];
 #pragma unroll
-      for (int r = 0; r < R; r++) uy[r] = uy0 + step_y * float(r);
+      for (int r = 0; r < R; r++)  // each row from its own index: independent of the tiling
+        uy[r] = float((sp.base_y + 2.0 * (sp.rhs_y * double(j0 + r * RS))) - lcy);
       // ---- near field, blocked compensated summation
       float sx[R], sy[R], cxr[R], cyr[R];
       float dxx[R], dxy[R];  // derivative sums (parity only)
@@ -342,7 +334,7 @@ __global__ void __launch_bounds__(kShootThreads) shoot_f32(ShootParams sp, LeafP
           py += (-a_sm.im - sp.kstar * z.im) * scy;
         }
         if (VERT) {
-          verts[(size_t)(j - sp.jbase) * (sp.nx) + i] = make_double2(px, double(sp.npy) - py);
+          o.verts[(size_t)(j - o.vrow0) * (sp.nx) + i] = make_double2(px, double(sp.npy) - py);
         } else {
           if (!(px >= 0.0 && px <= double(sp.npx) && py >= 0.0 && py <= double(sp.npy))) continue;
           bool pmin_ = false;
@@ -362,11 +354,50 @@ __global__ void __launch_bounds__(kShootThreads) shoot_f32(ShootParams sp, LeafP
             double mu = 1.0 / (dwdz * dwdz - (gr * gr + gi * gi));
             pmin_ = mu >= 0;
           }
-          irs_deposit(px, py, sp.npx, sp.npy, pix, pmin, psad, pmin_, PAR);
+          irs_deposit(px, py, sp.npx, sp.npy, o.pix, o.pmin, o.psad, pmin_, PAR);
         }
       }
     }
     __syncthreads();
+  }
+}
+
+template <bool VERT, bool PAR, bool GENERIC_SMOOTH>
+__global__ void __launch_bounds__(kShootThreads) shoot_f32(ShootParams sp, LeafPtrs lp, long long total_tiles,
+                                                           int* __restrict__ pix, int* __restrict__ pmin,
+                                                           int* __restrict__ psad, double2* __restrict__ verts) {
+  __shared__ float4 s_near[kMaxStarsDirect];
+  __shared__ float2 s_coef[kMaxOrder];
+  const ShootOut o{pix, pmin, psad, verts, sp.jbase};
+  for (long long t = blockIdx.x; t < total_tiles; t += gridDim.x)
+    shoot_f32_tile<VERT, PAR, GENERIC_SMOOTH>(sp, lp, tile_info(lp, t), o, s_near, s_coef);
+}
+
+// Many realizations in one launch: the tiles of all their leaves form one work
+// list; each tile takes the lens parameters of its leaf's realization and
+// writes into that realization's part of the corner buffer.
+struct BatchShoot {
+  const ShootParams* sps;    // per realization
+  const int* leaf_rid;       // per leaf
+  const long long* vrow0;    // per realization: first corner row held in the buffer
+  const long long* voff;     // per realization: offset of its rows in the buffer
+  const long long* total;    // number of tiles (device)
+  long long table_cap;       // entries the tile table holds
+  const int* err;            // error bits; a table overflow leaves the table unusable
+};
+
+template <bool GENERIC_SMOOTH>
+__global__ void __launch_bounds__(kShootThreads) shoot_f32_batch(BatchShoot bs, LeafPtrs lp,
+                                                                 double2* __restrict__ verts) {
+  __shared__ float4 s_near[kMaxStarsDirect];
+  __shared__ float2 s_coef[kMaxOrder];
+  if (*bs.err & kErrTableOverflow) return;
+  const long long total = *bs.total < bs.table_cap ? *bs.total : bs.table_cap;
+  for (long long t = blockIdx.x; t < total; t += gridDim.x) {
+    const TileInfo ti = tile_info(lp, t);
+    const int r = bs.leaf_rid[ti.leaf];
+    const ShootOut o{nullptr, nullptr, nullptr, verts + bs.voff[r], bs.vrow0[r]};
+    shoot_f32_tile<true, false, GENERIC_SMOOTH>(bs.sps[r], lp, ti, o, s_near, s_coef);
   }
 }
 

@@ -31,6 +31,20 @@
 
 namespace irsb {
 
+// Node range of one level: [beg, end) given by the host, or read on the device
+// from off[lvl], off[lvl + 1] when off is set (graph-captured builds, whose
+// level sizes are not known to the host).
+struct LevelRange {
+  const int* off = nullptr;
+  int lvl = 0;
+  __device__ __forceinline__ void get(int& beg, int& end) const {
+    if (off) {
+      beg = off[lvl];
+      end = off[lvl + 1];
+    }
+  }
+};
+
 template <typename T>
 struct TreeDev {
   int cap = 0;
@@ -39,6 +53,7 @@ struct TreeDev {
   std::vector<int> level_off;  // host copy, size levels + 2
   DevVec<T> cx, cy, hl;
   DevVec<int> level, parent, child0, sbeg, scnt;
+  DevVec<int> rid;         // realization of the node (0 for a single star field)
   DevVec<int> nbr, n_nbr;  // [cap][kMaxNeighbors]
   DevVec<int> sil, n_sil;  // [cap][kMaxSameLevelIL]
   DevVec<int> dil, n_dil;  // [cap][kMaxDiffLevelIL]
@@ -69,7 +84,7 @@ bool tree_reserve(TreeDev<T>& t, int want, cudaStream_t s) {
   int nc = t.cap ? t.cap : 1024;
   while (nc < want) nc *= 2;
   bool ok = t.cx.reserve(nc, s) && t.cy.reserve(nc, s) && t.hl.reserve(nc, s) && t.level.reserve(nc, s) &&
-            t.parent.reserve(nc, s) && t.child0.reserve(nc, s) && t.sbeg.reserve(nc, s) && t.scnt.reserve(nc, s) &&
+            t.parent.reserve(nc, s) && t.child0.reserve(nc, s) && t.sbeg.reserve(nc, s) && t.scnt.reserve(nc, s) && t.rid.reserve(nc, s) &&
             t.nbr.reserve(size_t(nc) * kMaxNeighbors, s) && t.n_nbr.reserve(nc, s) &&
             t.sil.reserve(size_t(nc) * kMaxSameLevelIL, s) && t.n_sil.reserve(nc, s) &&
             t.dil.reserve(size_t(nc) * kMaxDiffLevelIL, s) && t.n_dil.reserve(nc, s) && t.lox.reserve(nc, s) &&
@@ -77,7 +92,7 @@ bool tree_reserve(TreeDev<T>& t, int want, cudaStream_t s) {
   if (!ok) return false;
   // keep the logical sizes in step so that growth copies every live node
   for (auto* v : {&t.cx.n, &t.cy.n, &t.hl.n}) *v = nc;
-  t.level.n = t.parent.n = t.child0.n = t.sbeg.n = t.scnt.n = t.n_nbr.n = t.n_sil.n = t.n_dil.n = nc;
+  t.level.n = t.parent.n = t.child0.n = t.sbeg.n = t.scnt.n = t.n_nbr.n = t.n_sil.n = t.n_dil.n = t.rid.n = nc;
   t.lox.n = t.hix.n = t.loy.n = t.hiy.n = nc;
   t.nbr.n = size_t(nc) * kMaxNeighbors;
   t.sil.n = size_t(nc) * kMaxSameLevelIL;
@@ -88,8 +103,9 @@ bool tree_reserve(TreeDev<T>& t, int want, cudaStream_t s) {
 
 template <typename T>
 __global__ void tree_init_root(T* cx, T* cy, T* hl, int* level, int* parent, int* child0, int* sbeg, int* scnt,
-                               int* n_nbr, int* n_sil, int* n_dil, double* lox, double* hix, double* loy,
+                               int* rid, int* n_nbr, int* n_sil, int* n_dil, double* lox, double* hix, double* loy,
                                double* hiy, T root_hl, int nstars) {
+  rid[0] = 0;
   cx[0] = T(0);
   cy[0] = T(0);
   hl[0] = root_hl;
@@ -106,8 +122,10 @@ __global__ void tree_init_root(T* cx, T* cy, T* hl, int* level, int* parent, int
 }
 
 // Stars of a node and its neighbours; split flag; level maximum.
-__global__ void tree_near_count(int beg, int end, const int* __restrict__ scnt, const int* __restrict__ nbr,
-                                const int* __restrict__ n_nbr, int* __restrict__ split, int* __restrict__ dstat) {
+__global__ void tree_near_count(int beg, int end, LevelRange lr, const int* __restrict__ scnt,
+                                const int* __restrict__ nbr, const int* __restrict__ n_nbr, int* __restrict__ split,
+                                int* __restrict__ dstat) {
+  lr.get(beg, end);
   int local_max = 0;
   for (int k = beg + blockIdx.x * blockDim.x + threadIdx.x; k < end; k += gridDim.x * blockDim.x) {
     int c = scnt[k];
@@ -121,12 +139,18 @@ __global__ void tree_near_count(int beg, int end, const int* __restrict__ scnt, 
 }
 
 template <typename T>
-__global__ void tree_make_children(int beg, int end, int child_base, const int* __restrict__ split,
-                                   const long long* __restrict__ rank, T* cx, T* cy, T* hl, int* level, int* parent,
-                                   int* child0, int* sbeg, int* scnt, int* n_nbr, int* n_sil, int* n_dil,
-                                   double* lox, double* hix, double* loy, double* hiy) {
+__global__ void tree_make_children(int beg, int end, int child_base, LevelRange lr, const int* __restrict__ stop,
+                                   const int* __restrict__ split, const long long* __restrict__ rank, T* cx, T* cy,
+                                   T* hl, int* level, int* parent, int* child0, int* sbeg, int* scnt, int* rid,
+                                   int* n_nbr, int* n_sil, int* n_dil, double* lox, double* hix, double* loy,
+                                   double* hiy) {
+  if (lr.off) {
+    lr.get(beg, end);
+    child_base = end;
+  }
+  const bool halt = stop && *stop;
   for (int k = beg + blockIdx.x * blockDim.x + threadIdx.x; k < end; k += gridDim.x * blockDim.x) {
-    if (!split[k - beg]) {
+    if (halt || !split[k - beg]) {
       child0[k] = -1;
       continue;
     }
@@ -144,6 +168,7 @@ __global__ void tree_make_children(int beg, int end, int child_base, const int* 
       hl[c] = h;
       level[c] = level[k] + 1;
       parent[c] = k;
+      rid[c] = rid[k];
       child0[c] = -1;
       sbeg[c] = sbeg[k];
       scnt[c] = 0;
@@ -166,78 +191,86 @@ __device__ __forceinline__ int star_quadrant(T x, T y, T cx, T cy) {
   return 3;
 }
 
-// One block per level node; split nodes with stars partition their star range
-// into the 4 child ranges, keeping the relative order of stars (stable).
+// Blocks stride over the level's nodes; split nodes with stars partition their
+// star range into the 4 child ranges, keeping the relative order of stars
+// (stable).
 template <typename T>
-__global__ void __launch_bounds__(256) tree_partition_stars(int beg, const int* __restrict__ split,
+__global__ void __launch_bounds__(256) tree_partition_stars(int beg, int end, LevelRange lr,
+                                                            const int* __restrict__ stop,
+                                                            const int* __restrict__ split,
                                                             const T* __restrict__ cx, const T* __restrict__ cy,
                                                             const int* __restrict__ child0, int* sbeg, int* scnt,
                                                             StarRec<T>* __restrict__ stars,
                                                             StarRec<T>* __restrict__ tmp) {
-  int k = beg + blockIdx.x;
-  if (!split[blockIdx.x]) return;
-  int b = sbeg[k], n = scnt[k];
-  int c0 = child0[k];
+  lr.get(beg, end);
+  if (stop && *stop) return;
   __shared__ int cnt[4];
   __shared__ int warp_cnt[8][4];
   __shared__ int base[4];
-  if (threadIdx.x < 4) cnt[threadIdx.x] = 0;
-  __syncthreads();
-  T pcx = cx[k], pcy = cy[k];
-  int lc[4] = {0, 0, 0, 0};
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    StarRec<T> s = stars[b + i];
-    lc[star_quadrant(s.x, s.y, pcx, pcy)]++;
-  }
-  for (int q = 0; q < 4; q++)
-    if (lc[q]) atomicAdd(&cnt[q], lc[q]);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int acc = b;
-    for (int q = 0; q < 4; q++) {
-      base[q] = acc;
-      sbeg[c0 + q] = acc;
-      scnt[c0 + q] = cnt[q];
-      acc += cnt[q];
-    }
-  }
-  __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int start = 0; start < n; start += blockDim.x) {
-    int i = start + threadIdx.x;
-    int q = -1;
-    StarRec<T> s;
-    if (i < n) {
-      s = stars[b + i];
-      q = star_quadrant(s.x, s.y, pcx, pcy);
-    }
-    unsigned m[4];
-    for (int qq = 0; qq < 4; qq++) m[qq] = __ballot_sync(0xffffffffu, q == qq);
-    if (lane < 4) warp_cnt[w][lane] = __popc(m[lane]);
+  for (int k = beg + blockIdx.x; k < end; k += gridDim.x) {
+    if (!split[k - beg]) continue;  // uniform over the block
+    const int b = sbeg[k], n = scnt[k];
+    const int c0 = child0[k];
+    if (threadIdx.x < 4) cnt[threadIdx.x] = 0;
     __syncthreads();
-    if (q >= 0) {
-      int off = base[q];
-      for (int ww = 0; ww < w; ww++) off += warp_cnt[ww][q];
-      off += __popc(m[q] & ((1u << lane) - 1u));
-      tmp[off] = s;
+    const T pcx = cx[k], pcy = cy[k];
+    int lc[4] = {0, 0, 0, 0};
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      StarRec<T> st = stars[b + i];
+      lc[star_quadrant(st.x, st.y, pcx, pcy)]++;
+    }
+    for (int q = 0; q < 4; q++)
+      if (lc[q]) atomicAdd(&cnt[q], lc[q]);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = b;
+      for (int q = 0; q < 4; q++) {
+        base[q] = acc;
+        sbeg[c0 + q] = acc;
+        scnt[c0 + q] = cnt[q];
+        acc += cnt[q];
+      }
     }
     __syncthreads();
-    if (threadIdx.x < 4) {
-      int add = 0;
-      for (int ww = 0; ww < (int)(blockDim.x >> 5); ww++) add += warp_cnt[ww][threadIdx.x];
-      base[threadIdx.x] += add;
+    for (int start = 0; start < n; start += blockDim.x) {
+      int i = start + threadIdx.x;
+      int q = -1;
+      StarRec<T> st;
+      if (i < n) {
+        st = stars[b + i];
+        q = star_quadrant(st.x, st.y, pcx, pcy);
+      }
+      unsigned m[4];
+      for (int qq = 0; qq < 4; qq++) m[qq] = __ballot_sync(0xffffffffu, q == qq);
+      if (lane < 4) warp_cnt[w][lane] = __popc(m[lane]);
+      __syncthreads();
+      if (q >= 0) {
+        int off = base[q];
+        for (int ww = 0; ww < w; ww++) off += warp_cnt[ww][q];
+        off += __popc(m[q] & ((1u << lane) - 1u));
+        tmp[off] = st;
+      }
+      __syncthreads();
+      if (threadIdx.x < 4) {
+        int add = 0;
+        for (int ww = 0; ww < (int)(blockDim.x >> 5); ww++) add += warp_cnt[ww][threadIdx.x];
+        base[threadIdx.x] += add;
+      }
+      __syncthreads();
     }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) stars[b + i] = tmp[b + i];
     __syncthreads();
   }
-  for (int i = threadIdx.x; i < n; i += blockDim.x) stars[b + i] = tmp[b + i];
 }
 
 // set_neighbors (tree_node.cuh:183-267) for the nodes of one level (>= 1).
 template <typename T>
-__global__ void tree_set_neighbors(int beg, int end, const T* __restrict__ cx, const T* __restrict__ cy,
-                                   const T* __restrict__ hl, const int* __restrict__ parent,
+__global__ void tree_set_neighbors(int beg, int end, LevelRange lr, const T* __restrict__ cx,
+                                   const T* __restrict__ cy, const T* __restrict__ hl, const int* __restrict__ parent,
                                    const int* __restrict__ child0, const int* __restrict__ scnt, int* nbr,
                                    int* n_nbr, int* sil, int* n_sil, int* dil, int* n_dil, int* dstat) {
+  lr.get(beg, end);
   for (int k = beg + blockIdx.x * blockDim.x + threadIdx.x; k < end; k += gridDim.x * blockDim.x) {
     int p = parent[k];
     T h = hl[k];
@@ -299,7 +332,7 @@ bool build_tree(TreeDev<T>& t, StarRec<T>* stars, int nstars, T root_hl, cudaStr
   if (!t.tmp_stars.reserve(nstars, s)) return false;
   if (!t.dstat.reserve(2, s)) return false;
   tree_init_root<T><<<1, 1, 0, s>>>(t.cx.p, t.cy.p, t.hl.p, t.level.p, t.parent.p, t.child0.p, t.sbeg.p, t.scnt.p,
-                                    t.n_nbr.p, t.n_sil.p, t.n_dil.p, t.lox.p, t.hix.p, t.loy.p, t.hiy.p, root_hl,
+                                    t.rid.p, t.n_nbr.p, t.n_sil.p, t.n_dil.p, t.lox.p, t.hix.p, t.loy.p, t.hiy.p, root_hl,
                                     nstars);
   IRSB_LAUNCH_CK("tree_init_root");
   t.level_off.assign({0, 1});
@@ -312,7 +345,7 @@ bool build_tree(TreeDev<T>& t, StarRec<T>* stars, int nstars, T root_hl, cudaStr
     if (!t.split.reserve(nl, s) || !t.rank.reserve(nl + 1, s)) return false;
     IRSB_CKR(cudaMemsetAsync(t.dstat.p, 0, sizeof(int), s));
     int blocks = std::min(ceil_div(nl, 256), 148 * 8);
-    tree_near_count<<<blocks, 256, 0, s>>>(beg, end, t.scnt.p, t.nbr.p, t.n_nbr.p, t.split.p, t.dstat.p);
+    tree_near_count<<<blocks, 256, 0, s>>>(beg, end, LevelRange{}, t.scnt.p, t.nbr.p, t.n_nbr.p, t.split.p, t.dstat.p);
     IRSB_LAUNCH_CK("tree_near_count");
     if (!exclusive_scan<int>(t.split.p, nl, t.rank.p, t.scan, s)) return false;
     long long nsplit = 0;
@@ -336,15 +369,16 @@ bool build_tree(TreeDev<T>& t, StarRec<T>* stars, int nstars, T root_hl, cudaStr
     int child_base = end;
     int nnew = int(4 * nsplit);
     if (!tree_reserve(t, end + nnew, s)) return false;
-    tree_make_children<T><<<blocks, 256, 0, s>>>(beg, end, child_base, t.split.p, t.rank.p, t.cx.p, t.cy.p, t.hl.p,
-                                                 t.level.p, t.parent.p, t.child0.p, t.sbeg.p, t.scnt.p, t.n_nbr.p,
+    tree_make_children<T><<<blocks, 256, 0, s>>>(beg, end, child_base, LevelRange{}, nullptr, t.split.p, t.rank.p,
+                                                 t.cx.p, t.cy.p, t.hl.p, t.level.p, t.parent.p, t.child0.p, t.sbeg.p,
+                                                 t.scnt.p, t.rid.p, t.n_nbr.p,
                                                  t.n_sil.p, t.n_dil.p, t.lox.p, t.hix.p, t.loy.p, t.hiy.p);
     IRSB_LAUNCH_CK("tree_make_children");
-    tree_partition_stars<T><<<nl, 256, 0, s>>>(beg, t.split.p, t.cx.p, t.cy.p, t.child0.p, t.sbeg.p, t.scnt.p,
+    tree_partition_stars<T><<<nl, 256, 0, s>>>(beg, end, LevelRange{}, nullptr, t.split.p, t.cx.p, t.cy.p, t.child0.p, t.sbeg.p, t.scnt.p,
                                                stars, t.tmp_stars.p);
     IRSB_LAUNCH_CK("tree_partition_stars");
     int nb2 = std::min(ceil_div(nnew, 256), 148 * 8);
-    tree_set_neighbors<T><<<std::max(nb2, 1), 256, 0, s>>>(child_base, child_base + nnew, t.cx.p, t.cy.p, t.hl.p,
+    tree_set_neighbors<T><<<std::max(nb2, 1), 256, 0, s>>>(child_base, child_base + nnew, LevelRange{}, t.cx.p, t.cy.p, t.hl.p,
                                                            t.parent.p, t.child0.p, t.scnt.p, t.nbr.p, t.n_nbr.p,
                                                            t.sil.p, t.n_sil.p, t.dil.p, t.n_dil.p, t.dstat.p);
     IRSB_LAUNCH_CK("tree_set_neighbors");

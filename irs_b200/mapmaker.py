@@ -36,12 +36,14 @@ class _MapMaker:
                  random_seed: int = None, write_stars: bool = None, write_maps: bool = None,
                  write_parities: bool = None, write_histograms: bool = None, outfile_prefix: str = None,
                  verbose: int = 0, is_double: bool = False, expansion_order: int = None,
-                 precision: int = None):
+                 precision: int = None, _handle=None):
         self.is_double = bool(is_double)
         self.lib = _lib.load(self._kind, self.is_double)
         self._T = C.c_double if self.is_double else C.c_float
         self._np_T = np.float64 if self.is_double else np.float32
-        self.obj = self.lib.init()
+        # _handle: an object owned elsewhere (the base map of an adaptive run)
+        self._owned = _handle is None
+        self.obj = self.lib.init() if _handle is None else _handle
         self.verbose = verbose
         self._host_stars = None
 
@@ -84,7 +86,8 @@ class _MapMaker:
     # ------------------------------------------------------------ lifetime
     def close(self):
         if getattr(self, "obj", None):
-            self.lib.destroy(self.obj)
+            if getattr(self, "_owned", True):
+                self.lib.destroy(self.obj)
             self.obj = None
 
     def __del__(self):
