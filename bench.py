@@ -283,6 +283,71 @@ def batch_measure(steps):
     return res
 
 
+ADAPTIVE_CONFIG = dict(kappa_tot=0.6, shear=0.3, smooth_fraction=0.3, mass_function="salpeter", m_lower=0.08,
+                       m_upper=1.0, theta_star=1.0, half_length_y1=30.0, half_length_y2=30.0, num_pixels_y1=4096,
+                       num_pixels_y2=4096, random_seed=4, write_histograms=0)
+
+
+def adaptive_measure():
+    """The learned-adaptive form on its configuration (4096^2 map): the
+    network-chosen map against the uniform-fine (level 16) map; the uniform
+    level whose map error matches it; and the plain uniform FP64 form at that
+    level (num_rays_y = level^2 cells per pixel area), its tree and
+    expansions timed once and its shooting timed on a band of lattice rows and
+    scaled to the lattice."""
+    import irs_b200
+
+    def rel_err(mu, ref):
+        ok = ref > 0
+        r = np.abs(mu[ok].astype(np.float64) - ref[ok]) / ref[ok]
+        return float(np.median(r)), float(np.quantile(r, 0.99))
+
+    cfg = ADAPTIVE_CONFIG
+    a = irs_b200.AdaptiveIPM(**cfg)
+    a.run()
+    a.run()  # the second run is timed (warm)
+    t_ada = a.value("t_base") + a.value("t_adapt")
+    mu_a = a.magnifications
+    lv = a.levels()
+    res = {"tiles": int(len(lv)), "levels_hist": np.bincount(np.log2(lv).astype(int), minlength=5).tolist(),
+           "cells_base": int(a.value("cells_base")), "cells_evaluated": int(a.value("cells_evaluated")),
+           "audited": int(a.value("audited")), "audit_failures": int(a.value("audit_failures")),
+           "t_base_ms": a.value("t_base") * 1e3, "t_adapt_ms": a.value("t_adapt") * 1e3}
+    a.close()
+    u16 = irs_b200.AdaptiveIPM(policy="uniform", level=16, audit_fraction=0.0, **cfg)
+    u16.run()
+    ref = u16.magnifications.astype(np.float64)
+    res["uniform16_ms"] = (u16.value("t_base") + u16.value("t_adapt")) * 1e3
+    u16.close()
+    med_a, p99_a = rel_err(mu_a, ref)
+    res.update({"median_rel_err_vs_uniform16": med_a, "p99_rel_err_vs_uniform16": p99_a})
+    match = 16
+    for L in (1, 2, 4, 8):
+        u = irs_b200.AdaptiveIPM(policy="uniform", level=L, audit_fraction=0.0, **cfg)
+        u.run()
+        med, _ = rel_err(u.magnifications, ref)
+        res[f"uniform{L}_median_rel_err"] = med
+        u.close()
+        if med <= med_a and match == 16:
+            match = L
+    res["uniform_level_matching_error"] = match
+    p = irs_b200.IPM(**{**cfg, "num_rays_y": match * match}, is_double=True)
+    p.derive()
+    ny = int(p.value("num_ray_threads_2"))
+    rows = max(1, ny // 16)
+    p.lib.set_band(p.obj, 0, rows)
+    p.run()
+    tb = p.rerun(1)
+    shoot = p.value("t_lattice") + p.value("t_deposit")
+    t_plain = (tb - shoot) + shoot * ny / rows  # tree and expansions once, shooting for every row
+    p.close()
+    res.update({"plain_fp64_s_at_matching_level": t_plain, "adaptive_s": t_ada,
+                "effective_cells_per_s_adaptive": res["cells_base"] * match * match / t_ada,
+                "effective_cells_per_s_plain_fp64": res["cells_base"] * match * match / t_plain,
+                "adaptive_over_plain_fp64": t_plain / t_ada})
+    return res
+
+
 def our_arm(args):
     import torch
 
@@ -402,6 +467,7 @@ def our_arm(args):
                           "rays_received": int(r.num_rays_received)}
             r.close()
         extra["batched_256"] = batch_measure(args.steps)
+        extra["learned_adaptive"] = adaptive_measure()
 
     if rank == 0:
         cpu = cpu_baseline(m, stars.astype(np.float64), os.cpu_count() or 1) if (ws == 1 and not args.no_cpu) else None

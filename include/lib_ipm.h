@@ -110,6 +110,9 @@ void set_stars(IPMHandle* self, const IPM_DTYPE* xym, int n, int rectangular, IP
 double get_t_pipeline(IPMHandle* self);               /* seconds: tree + expansions + shoot */
 bool rerun(IPMHandle* self, int repeats, double* seconds); /* re-run tree+expansions+shoot on the resident stars */
 void set_band(IPMHandle* self, long long first, long long last); /* lattice row band [first, last); last < 0: all */
+void set_shoot_launch(IPMHandle* self, int threads, int ctas_per_sm); /* FP32 lens-equation kernel: 128/256/512 threads per CTA (8/4/2 lattice points per thread), CTAs per SM */
+int get_shoot_threads(IPMHandle* self);
+int get_shoot_ctas_per_sm(IPMHandle* self);
 bool copy_maps_device(IPMHandle* self, void* total, void* minima, void* saddles); /* integer maps to device buffers */
 bool derive(IPMHandle* self);                          /* validate + derived parameters, no GPU work */
 double get_value(IPMHandle* self, const char* name);   /* derived / run-time value by name, NaN if unknown */
@@ -156,6 +159,39 @@ bool batch_copy_maps(void* batch, IPM_DTYPE* out);           /* [size][npy][npx]
 const IPM_DTYPE* batch_maps_device(void* batch);             /* the same maps on the device */
 bool batch_copy_stars(void* batch, IPM_DTYPE* out);          /* all star fields, tree order, (x1, x2, m) */
 double batch_get_value(void* batch, int r, const char* name); /* r >= 0: realization value; r < 0: batch value */
+
+/* Adaptive IPM (no counterpart in the reference): the cell lattice is cut into
+ * 32 x 32-cell tiles, each deposited at a subdivision level 1, 2, 4, 8 or 16
+ * chosen by the level network (or uniform / given levels); every run audits a
+ * seeded random sample of tiles against level 16 and sends a tile that misses
+ * the tolerance to level 16. Map inputs are set on the object from ada_base. */
+void* ada_init(void);
+void ada_destroy(void* ada);
+IPMHandle* ada_base(void* ada);                                   /* the map's inputs (setters of this library) */
+void ada_set_policy(void* ada, int policy, int uniform_level);    /* 0 network, 1 uniform level, 2 given levels */
+void ada_set_levels(void* ada, const int* levels, int n);         /* policy 2: one level per tile, row-major */
+void ada_set_tolerance(void* ada, double eps);                    /* share of a tile's flux put in wrong pixels */
+void ada_set_quantile(void* ada, float q);                        /* network: smallest level with cumulative p >= q */
+void ada_set_audit(void* ada, double fraction, unsigned seed);
+void ada_set_refine_capacity(void* ada, long long corners);       /* refinement buffer, 0: automatic */
+void ada_set_network(void* ada, const float* w, const float* mu, const float* sig); /* 5061 weights, 8 + 8 */
+bool ada_run(void* ada, int verbose);
+int ada_num_tiles(void* ada);
+bool ada_copy_features(void* ada, float* out);                   /* [tiles][8] */
+bool ada_copy_levels(void* ada, int* out, int predicted);        /* final (after audit) or predicted levels */
+bool ada_labels(void* ada, const int* tiles, int n, int* labels, float* err); /* classes 0..4, errors [n][4] */
+bool ada_copy_map(void* ada, IPM_DTYPE* out);
+double ada_get_value(void* ada, const char* name);
+
+/* The level network alone (8 -> 64 -> 64 -> 5, BF16 weights, FP32
+ * accumulation; no counterpart in the reference): device training with Adam,
+ * gradients of the mean cross-entropy, argmax prediction. */
+int mlp_num_params(void);
+bool mlp_train(const float* feat, const int* labels, int n, int epochs, int batch, float lr, unsigned seed, float* w,
+               float* mu, float* sig, float* epoch_loss);
+bool mlp_gradients(const float* w, const float* mu, const float* sig, const float* feat, const int* labels, int n,
+                   float* grad, float* mean_loss);
+bool mlp_predict(const float* w, const float* mu, const float* sig, const float* feat, int n, int* cls);
 
 #ifdef __cplusplus
 }

@@ -40,14 +40,15 @@ REFERENCE_IPM_SYMBOLS = (
 )
 EXTENSION_SYMBOLS = [
     "destroy", "set_expansion_order", "get_expansion_order", "set_precision", "get_precision",
-    "set_stars", "get_t_pipeline", "rerun", "set_band", "copy_maps_device", "derive", "get_value", "get_tree_num_nodes", "copy_tree",
+    "set_stars", "get_t_pipeline", "rerun", "set_band", "set_shoot_launch", "get_shoot_threads",
+    "get_shoot_ctas_per_sm", "copy_maps_device", "derive", "get_value", "get_tree_num_nodes", "copy_tree",
     "copy_coeffs", "get_num_vertices", "copy_vertices", "copy_fixed_maps",
 ]
 IRS_ONLY_SYMBOLS = ["get_t_shoot_rays", "get_num_rays_shot", "get_num_rays_received"]
 IPM_ONLY_SYMBOLS = ["ipm_deposit_noalloc", "batch_init", "batch_destroy", "batch_add", "batch_size",
                     "batch_set_expansion_order", "batch_set_corner_capacity", "batch_run", "batch_rerun",
                     "batch_copy_maps", "batch_maps_device", "batch_copy_stars", "batch_get_value",
-                    "ada_init", "ada_destroy", "ada_base", "ada_set_policy", "ada_set_levels", "ada_set_tolerance",
+                    "ada_init", "ada_destroy", "ada_base", "ada_set_policy", "ada_set_levels", "ada_set_tolerance", "ada_set_quantile",
                     "ada_set_audit", "ada_set_refine_capacity", "ada_set_network", "ada_run", "ada_num_tiles",
                     "ada_copy_features", "ada_copy_levels", "ada_labels", "ada_copy_map", "ada_get_value",
                     "mlp_num_params", "mlp_train", "mlp_gradients", "mlp_predict"]
@@ -131,6 +132,12 @@ def _bind(lib, kind: str, is_double: bool):
     lib.rerun.restype = C.c_bool
     lib.set_band.argtypes = [vp, C.c_longlong, C.c_longlong]
     lib.set_band.restype = None
+    lib.set_shoot_launch.argtypes = [vp, C.c_int, C.c_int]
+    lib.set_shoot_launch.restype = None
+    lib.get_shoot_threads.argtypes = [vp]
+    lib.get_shoot_threads.restype = C.c_int
+    lib.get_shoot_ctas_per_sm.argtypes = [vp]
+    lib.get_shoot_ctas_per_sm.restype = C.c_int
     lib.copy_maps_device.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.copy_maps_device.restype = C.c_bool
     lib.derive.argtypes = [vp]
@@ -178,7 +185,8 @@ def _bind(lib, kind: str, is_double: bool):
         for name, args, res in [
                 ("ada_init", [], vp), ("ada_destroy", [vp], None), ("ada_base", [vp], vp),
                 ("ada_set_policy", [vp, C.c_int, C.c_int], None), ("ada_set_levels", [vp, ip, C.c_int], None),
-                ("ada_set_tolerance", [vp, C.c_double], None), ("ada_set_audit", [vp, C.c_double, C.c_uint], None),
+                ("ada_set_tolerance", [vp, C.c_double], None), ("ada_set_quantile", [vp, C.c_float], None),
+                ("ada_set_audit", [vp, C.c_double, C.c_uint], None),
                 ("ada_set_refine_capacity", [vp, C.c_longlong], None), ("ada_set_network", [vp, fp, fp, fp], None),
                 ("ada_run", [vp, C.c_int], C.c_bool), ("ada_num_tiles", [vp], C.c_int),
                 ("ada_copy_features", [vp, fp], C.c_bool), ("ada_copy_levels", [vp, ip, C.c_int], C.c_bool),

@@ -5,9 +5,10 @@ is deposited at a subdivision level 1, 2, 4, 8 or 16 (subcells per cell side).
 `LevelNet` (8 -> 64 -> 64 -> 5, BF16 weights, FP32 accumulation) predicts the
 level from per-tile features; it is trained on the device by the library's
 own forward/backward kernels on labels the method generates itself (the
-smallest level whose interpolation stays within a tolerance of the level-16
-positions). Every run audits a seeded random sample of tiles at level 16 and
-sends a tile whose chosen level exceeds the tolerance to level 16.
+smallest level at which a tile's own deposit is within a tolerance of its
+level-16 deposit, as a share of the tile's flux). Every run audits a seeded
+random sample of tiles against level 16 and sends a tile whose chosen level
+misses the tolerance to level 16.
 """
 from __future__ import annotations
 
@@ -20,8 +21,8 @@ from . import _lib
 from .mapmaker import IPM
 
 LEVELS = (1, 2, 4, 8, 16)
-FEATURES = ("kappa_smooth", "kappa_star", "shear_local", "log_det_min", "log_det_max", "critical", "log_star_dist",
-            "log_edge_max")
+FEATURES = ("kappa_smooth", "kappa_star_local", "shear_local", "log_det_min", "log_det_max", "critical",
+            "log_star_dist", "log_map_dist")
 DEFAULT_NET = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "level_net.npz")
 
 
@@ -87,12 +88,15 @@ class AdaptiveIPM:
     """An IPM map with per-tile subdivision.
 
     policy: "network" (levels from `network`), "uniform" (every tile at
-    `level`) or "given" (per-tile `levels`). tolerance: interpolation error in
-    pixels that a tile's level must meet (labels and audit). The map inputs
+    `level`) or "given" (per-tile `levels`). tolerance: share of a tile's flux
+    that its level may put in other pixels than level 16 does (labels and
+    audit). quantile: a tile takes the smallest level whose cumulative network
+    probability reaches it (above 0.5 leans towards refining). The map inputs
     are those of IPM (keyword arguments)."""
 
-    def __init__(self, network=None, policy="network", level=1, levels=None, tolerance=5e-4,
-                 audit_fraction=0.01, audit_seed=1, refine_capacity=0, is_double=False, verbose=0, **ipm_kwargs):
+    def __init__(self, network=None, policy="network", level=1, levels=None, tolerance=1e-3,
+                 audit_fraction=0.01, audit_seed=1, refine_capacity=0, quantile=0.8, is_double=False, verbose=0,
+                 **ipm_kwargs):
         self.is_double = bool(is_double)
         self.lib = _lib.load("ipm", self.is_double)
         self._np_T = np.float64 if self.is_double else np.float32
@@ -110,6 +114,7 @@ class AdaptiveIPM:
             lv = np.ascontiguousarray(levels, np.int32)
             self.lib.ada_set_levels(self.h, _fp(lv), len(lv))
         self.lib.ada_set_tolerance(self.h, float(tolerance))
+        self.lib.ada_set_quantile(self.h, float(quantile))
         self.lib.ada_set_audit(self.h, float(audit_fraction), int(audit_seed))
         self.lib.ada_set_refine_capacity(self.h, int(refine_capacity))
 
@@ -151,7 +156,7 @@ class AdaptiveIPM:
         return out
 
     def labels(self, tiles):
-        """(classes 0..4, interpolation errors of levels 1, 2, 4, 8 [n, 4])."""
+        """(classes 0..4, deposit errors of levels 1, 2, 4, 8 against 16 [n, 4])."""
         t = np.ascontiguousarray(tiles, np.int32)
         lab = np.zeros(len(t), np.int32)
         err = np.zeros((len(t), 4), np.float32)

@@ -22,11 +22,11 @@
 //     global fine index, so neighbouring tiles compute shared points
 //     identically.
 //
-// Labels for training: a tile's label is the smallest level s whose
-// piecewise-linear interpolation over its cells' two triangles (the shape the
-// deposition gives each triangle) misplaces at most a share eps of the
-// tile's flux against the level-16 positions (ada_level_errors; 16 when no
-// coarser level does).
+// Labels for training: a tile's label is the smallest level s whose deposit
+// differs from the tile's level-16 deposit by at most a share eps of its flux
+// (relative L1 over the tile's own pixel window; 16 when no coarser level
+// does): the level at which the tile's deposit converges to the uniform-fine
+// map.
 #pragma once
 #include "deposit.cuh"
 #include "leaves.cuh"
@@ -139,13 +139,6 @@ struct AdaGeom {
   int npx, npy;                         // map
 };
 
-// A source position (pixels) that can reach the map: inside it or within
-// kAdaMargin pixels of its border.
-constexpr double kAdaMargin = 2.0;
-__device__ __forceinline__ bool ada_on_map(const AdaGeom& g, double2 p) {
-  return p.x >= -kAdaMargin && p.x <= g.npx + kAdaMargin && p.y >= -kAdaMargin && p.y <= g.npy + kAdaMargin;
-}
-
 // Corner (a, b) of tile t at level s, in the tile's corner grid
 // [0, ncell_x * s] x [0, ncell_y * s].
 template <typename T, bool GENERIC_SMOOTH>
@@ -223,86 +216,110 @@ __global__ void __launch_bounds__(256) ada_refine_corners(AdaGeom g, ShootParams
   }
 }
 
-// Interpolation error of levels 1, 2, 4, 8 against the level-16 corner grid
-// of each tile in `list` (grid at fine + slot * stride, row stride
-// ncell_x * 16 + 1), as the share of deposited flux that the coarser level
-// misplaces: at every fine corner where either position can reach the map,
-// the distance (pixels) between the level-16 position and the piecewise-linear
-// interpolation of level 2^c over the two triangles of the level-2^c cell
-// containing it, divided by that cell's image size (its longest edge, at
-// least one pixel: a displacement moves about distance / size of an image
-// larger than a pixel across pixel borders, and about the distance itself of
-// a smaller one). err[slot * 4 + c] is the mean over those corners; every
-// cell carries the same flux, so the mean weights them equally. Near a star
-// the lens map runs off with diverging curvature, but its images there are
-// stretched, so the relative measure keeps those corners in proportion.
-// One block per tile.
-__global__ void __launch_bounds__(256) ada_level_errors(AdaGeom g, const int* __restrict__ list, int nlist,
+// Deposit error of levels 1, 2, 4, 8 against level 16, tile by tile. Each
+// tile is deposited on its own into a private pixel window at every level
+// (level-s corners are every (16/s)-th level-16 corner), and
+//   err[slot * 4 + c] = sum |W_c - W_16| / (2 factor * cells of the tile)
+// over the window, W_c being the tile's deposit at level 2^c: the share of
+// the tile's flux that level 2^c puts in the wrong pixels.
+constexpr int kAdaWindow = 256;       // pixels per side of a tile's window
+constexpr int kAdaWindowLarge = 1024; // window of a chunk holding a tile whose image needs more
+constexpr int kAdaWindowMargin = 2;
+
+// Window of each tile: the pixel bounding box of its level-16 image within the
+// map, widened by kAdaWindowMargin; win[slot] = (x0, y0, w, h), w = 0 when the
+// image misses the map, w = -1 when the box exceeds the large window.
+__global__ void __launch_bounds__(256) ada_tile_windows(AdaGeom g, const int* __restrict__ list, int nlist,
                                                         long long stride, const double2* __restrict__ fine,
-                                                        float* __restrict__ err) {
-  __shared__ double red_s[4][8];
-  __shared__ int red_n[4][8];
+                                                        int4* __restrict__ win) {
+  __shared__ double red[4][8];
   for (int slot = blockIdx.x; slot < nlist; slot += gridDim.x) {
     const int t = list[slot];
     const int tx = t % g.ntx, ty = t / g.ntx;
     const int ncx_t = int(llmin_(kAdaTile, g.ncx - (long long)tx * kAdaTile));
     const int ncy_t = int(llmin_(kAdaTile, g.ncy - (long long)ty * kAdaTile));
-    const int W = ncx_t * kAdaMaxLevel + 1, H = ncy_t * kAdaMaxLevel + 1;
+    const int n = (ncx_t * kAdaMaxLevel + 1) * (ncy_t * kAdaMaxLevel + 1);
     const double2* P = fine + (long long)slot * stride;
-    double sum[4] = {0, 0, 0, 0};
-    int cnt[4] = {0, 0, 0, 0};
-    for (int q = threadIdx.x; q < W * H; q += blockDim.x) {
-      const int b = q / W, a = q - b * W;
+    double m[4] = {1e300, 1e300, -1e300, -1e300};  // xmin, ymin, xmax, ymax
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
       const double2 v = P[q];
-#pragma unroll
-      for (int c = 0; c < 4; c++) {
-        const int step = kAdaMaxLevel >> c;  // fine corners per level-2^c cell side
-        int a0 = (a / step) * step, b0 = (b / step) * step;
-        if (a0 == W - 1) a0 -= step;
-        if (b0 == H - 1) b0 -= step;
-        const double u = double(a - a0) / step, w = double(b - b0) / step;
-        // cell corners: y2 = (a0, b0), y3 = (a1, b0), y0 = (a1, b1), y1 = (a0, b1);
-        // triangles (y0, y1, y2) for u <= w and (y2, y3, y0) for u >= w
-        const double2 p2 = P[(long long)b0 * W + a0], p0 = P[(long long)(b0 + step) * W + a0 + step];
-        const double2 p1 = P[(long long)(b0 + step) * W + a0], p3 = P[(long long)b0 * W + a0 + step];
-        double2 r;
-        if (u <= w)
-          r = make_double2(p2.x + w * (p1.x - p2.x) + u * (p0.x - p1.x), p2.y + w * (p1.y - p2.y) + u * (p0.y - p1.y));
-        else
-          r = make_double2(p2.x + u * (p3.x - p2.x) + w * (p0.x - p3.x), p2.y + u * (p3.y - p2.y) + w * (p0.y - p3.y));
-        if (ada_on_map(g, v) || ada_on_map(g, r)) {
-          const double size = fmax(fmax(hypot(p3.x - p2.x, p3.y - p2.y), hypot(p1.x - p2.x, p1.y - p2.y)),
-                                   fmax(hypot(p0.x - p1.x, p0.y - p1.y), hypot(p0.x - p3.x, p0.y - p3.y)));
-          const double e = hypot(r.x - v.x, r.y - v.y) / fmax(size, 1.0);
-          if (!isnan(e)) {
-            sum[c] += e;
-            cnt[c]++;
-          }
-        }
-      }
+      if (!(fabs(v.x) < 1e12 && fabs(v.y) < 1e12)) continue;
+      m[0] = fmin(m[0], v.x);
+      m[1] = fmin(m[1], v.y);
+      m[2] = fmax(m[2], v.x);
+      m[3] = fmax(m[3], v.y);
     }
 #pragma unroll
     for (int c = 0; c < 4; c++) {
-      double v = sum[c];
-      int k = cnt[c];
+      double v = m[c];
       for (int o = 16; o > 0; o >>= 1) {
-        v += __shfl_down_sync(0xffffffffu, v, o);
-        k += __shfl_down_sync(0xffffffffu, k, o);
+        const double u = __shfl_down_sync(0xffffffffu, v, o);
+        v = c < 2 ? fmin(v, u) : fmax(v, u);
       }
-      if ((threadIdx.x & 31) == 0) {
-        red_s[c][threadIdx.x >> 5] = v;
-        red_n[c][threadIdx.x >> 5] = k;
+      if ((threadIdx.x & 31) == 0) red[c][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double r[4] = {red[0][0], red[1][0], red[2][0], red[3][0]};
+      for (int w = 1; w < int(blockDim.x >> 5); w++) {
+        r[0] = fmin(r[0], red[0][w]);
+        r[1] = fmin(r[1], red[1][w]);
+        r[2] = fmax(r[2], red[2][w]);
+        r[3] = fmax(r[3], red[3][w]);
       }
+      const double x0 = fmax(floor(r[0]) - kAdaWindowMargin, 0.0), y0 = fmax(floor(r[1]) - kAdaWindowMargin, 0.0);
+      const double x1 = fmin(ceil(r[2]) + kAdaWindowMargin, double(g.npx));
+      const double y1 = fmin(ceil(r[3]) + kAdaWindowMargin, double(g.npy));
+      int4 o = make_int4(0, 0, 0, 0);
+      if (x1 > x0 && y1 > y0) {
+        o = make_int4(int(x0), int(y0), int(x1 - x0), int(y1 - y0));
+        if (o.z > kAdaWindowLarge || o.w > kAdaWindowLarge) o.z = -1;
+      }
+      win[slot] = o;
+    }
+    __syncthreads();
+  }
+}
+
+// Differences of the resolved windows of side ws (window of slot k, level c
+// at acc + (k * 5 + c) * ws^2) as a share of the tile's whole flux (2 factor
+// per cell, on the map or not), so that a tile with little flux on the map
+// cannot have a large error.
+__global__ void __launch_bounds__(256) ada_window_errors(AdaGeom g, const int* __restrict__ list, int nlist, int ws,
+                                                         float factor, const int4* __restrict__ win,
+                                                         const unsigned long long* __restrict__ acc,
+                                                         float* __restrict__ err) {
+  __shared__ double red[5][8];
+  const long long W2 = (long long)ws * ws;
+  for (int slot = blockIdx.x; slot < nlist; slot += gridDim.x) {
+    const int4 w = win[slot];
+    if (w.z <= 0) {  // uniform over the block
+      if (threadIdx.x < 4) err[(long long)slot * 4 + threadIdx.x] = w.z < 0 ? 1.f : 0.f;
+      continue;
+    }
+    const unsigned long long* A = acc + (long long)slot * 5 * W2;
+    double d[4] = {0, 0, 0, 0}, tot = 0;
+    for (long long q = threadIdx.x; q < W2; q += blockDim.x) {
+      const long long a16 = (long long)A[4 * W2 + q];
+      tot += double(a16);
+#pragma unroll
+      for (int c = 0; c < 4; c++) d[c] += fabs(double((long long)A[c * W2 + q] - a16));
+    }
+#pragma unroll
+    for (int c = 0; c < 5; c++) {
+      double v = c < 4 ? d[c] : tot;
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if ((threadIdx.x & 31) == 0) red[c][threadIdx.x >> 5] = v;
     }
     __syncthreads();
     if (threadIdx.x < 4) {
-      double v = 0;
-      long long k = 0;
-      for (int w = 0; w < int(blockDim.x >> 5); w++) {
-        v += red_s[threadIdx.x][w];
-        k += red_n[threadIdx.x][w];
-      }
-      err[(long long)slot * 4 + threadIdx.x] = k ? float(v / double(k)) : 0.f;
+      const int t = list[slot];
+      const long long cells = llmin_(kAdaTile, g.ncx - (long long)(t % g.ntx) * kAdaTile) *
+                              llmin_(kAdaTile, g.ncy - (long long)(t / g.ntx) * kAdaTile);
+      const double whole = double(cells) * 2.0 * double(factor) * kFixScale;
+      double num = 0;
+      for (int k = 0; k < int(blockDim.x >> 5); k++) num += red[threadIdx.x][k];
+      err[(long long)slot * 4 + threadIdx.x] = float(num / whole);
     }
     __syncthreads();
   }
@@ -311,7 +328,9 @@ __global__ void __launch_bounds__(256) ada_level_errors(AdaGeom g, const int* __
 // Per-tile features from the base corner lattice and the tree (one thread per
 // tile):
 //   0  smooth convergence kappa_tot - kappa_star
-//   1  star convergence kappa_star
+//   1  local star convergence: theta^2 sum m of the near field of the leaf
+//      that owns the tile centre over its area / pi (the leaf and its
+//      neighbours, (6 hl)^2)
 //   2  mean shear magnitude of the local Jacobian at the tile's 4 corner cells
 //   3  log10 of the smallest |det J| at those cells (J = d source / d lens, in
 //      pixels per unlensed pixel, from the cell's edge vectors)
@@ -320,7 +339,8 @@ __global__ void __launch_bounds__(256) ada_level_errors(AdaGeom g, const int* __
 //      through the tile), else 0
 //   6  log10 of the distance from the tile centre to the nearest star of the
 //      leaf that owns the centre (its near field), in cell widths
-//   7  log10 of the largest image edge length (pixels) of those cells
+//   7  log10(1 + distance in pixels from the bounding box of the images of
+//      the tile's 4 corners to the map), 0 when they overlap the map
 template <typename T>
 __global__ void ada_features(AdaGeom g, ShootParams sp, LeafPtrs lp, DescentPtrs<T> dp,
                              const double2* __restrict__ base_verts, float* __restrict__ feat) {
@@ -331,7 +351,7 @@ __global__ void ada_features(AdaGeom g, ShootParams sp, LeafPtrs lp, DescentPtrs
     const long long i0 = (long long)tx * kAdaTile, j0 = (long long)ty * kAdaTile;
     const long long ilast = llmin_(i0 + kAdaTile, g.ncx) - 1, jlast = llmin_(j0 + kAdaTile, g.ncy) - 1;
     const long long ci[4] = {i0, ilast, i0, ilast}, cj[4] = {j0, j0, jlast, jlast};
-    double gsum = 0, dmin = 1e300, dmax = 0, emax = 0;
+    double gsum = 0, dmin = 1e300, dmax = 0;
     int npos = 0, nneg = 0;
     for (int k = 0; k < 4; k++) {
       const long long i = ci[k], j = cj[k], vx = g.ncx + 1;
@@ -348,7 +368,6 @@ __global__ void ada_features(AdaGeom g, ShootParams sp, LeafPtrs lp, DescentPtrs
       dmax = fmax(dmax, ad);
       if (det >= 0) npos++;
       else nneg++;
-      emax = fmax(emax, fmax(hypot(p10.x - p00.x, p10.y - p00.y), hypot(p01.x - p00.x, p01.y - p00.y)));
     }
     // nearest star of the near field at the tile centre
     const double xc = g.base_x + 2.0 * (g.rhs_x * (double(i0) + 0.5 * double(ilast - i0 + 1)));
@@ -362,15 +381,34 @@ __global__ void ada_features(AdaGeom g, ShootParams sp, LeafPtrs lp, DescentPtrs
       dn = fmin(dn, hypot(xc - (lcx + double(st.x)), yc - (lcy + double(st.y))));
     }
     if (nn == 0) dn = 2.0 * lp.hl[leaf];
+    double msum = 0;  // near32 holds m theta^2
+    for (int s = 0; s < nn; s++) msum += lp.near32[(size_t)leaf * kMaxStarsDirect + s].z;
+    const double hl = lp.hl[leaf];
+    const double kloc = msum * 3.14159265358979323846 / (36.0 * hl * hl);
+    // image of the tile's corners against the map
+    double bx0 = 1e300, by0 = 1e300, bx1 = -1e300, by1 = -1e300;
+    {
+      const long long vx = g.ncx + 1;
+      const long long qi[4] = {i0, ilast + 1, i0, ilast + 1}, qj[4] = {j0, j0, jlast + 1, jlast + 1};
+      for (int k = 0; k < 4; k++) {
+        const double2 q = base_verts[qj[k] * vx + qi[k]];
+        bx0 = fmin(bx0, q.x);
+        bx1 = fmax(bx1, q.x);
+        by0 = fmin(by0, q.y);
+        by1 = fmax(by1, q.y);
+      }
+    }
+    const double ddx = fmax(0.0, fmax(bx0 - double(g.npx), -bx1)), ddy = fmax(0.0, fmax(by0 - double(g.npy), -by1));
+    const double dmap = hypot(ddx, ddy);
     float* f = feat + (long long)t * kAdaFeatures;
     f[0] = float(sp.kappa - sp.kstar);
-    f[1] = float(sp.kstar);
+    f[1] = float(kloc);
     f[2] = float(gsum * 0.25);
     f[3] = float(log10(dmin + 1e-6));
     f[4] = float(log10(dmax + 1e-6));
     f[5] = (npos > 0 && nneg > 0) ? 1.f : 0.f;
     f[6] = float(log10(dn / (2.0 * sp.rhs_x) + 1e-6));
-    f[7] = float(log10(emax + 1e-6));
+    f[7] = isfinite(dmap) ? float(log10(1.0 + dmap)) : 12.f;
   }
 }
 

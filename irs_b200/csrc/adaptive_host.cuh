@@ -5,9 +5,9 @@
 //      lattice (tree, expansions, leaf records, tiled lens equation);
 //   2. per-tile features and the level of every tile: from the network, one
 //      uniform level, or levels given by the caller;
-//   3. audit: a seeded random sample of tiles is evaluated at level 16 and the
-//      flux share misplaced by its chosen level measured (ada_level_errors); a
-//      tile above the tolerance falls back to level 16;
+//   3. audit: a seeded random sample of tiles is deposited on its own at its
+//      chosen level and at level 16 (ada_window_errors); a tile whose deposit
+//      differs by more than the tolerance falls back to level 16;
 //   4. deposition: level-1 tiles straight from the base lattice, refined tiles
 //      level by level through a bounded corner buffer (conforming corners,
 //      factor / s^2 per subcell), all into one fixed-point map;
@@ -34,11 +34,12 @@ class AdaptiveIPM {
   int policy = kAdaNetwork;
   int uniform_level = 1;
   std::vector<int> given_levels;
-  double eps = 5e-4;             // tolerance: share of a tile's flux that its level may misplace
+  double eps = 1e-3;             // tolerance: share of a tile's flux its level may put in wrong pixels
   double audit_fraction = 0.01;  // share of tiles audited per run
   unsigned audit_seed = 1;
   long long refine_cap = 0;      // corner positions in the refinement buffer (0: automatic)
   std::vector<float> net_w, net_mu, net_sig;  // FP32 master weights, feature standardisation
+  float net_quantile = 0.8f;  // a tile takes the smallest level whose cumulative probability reaches this
 
   // results
   int ntx = 0, nty = 0;
@@ -86,7 +87,7 @@ class AdaptiveIPM {
   }
 
   // Labels of `tiles` (after run): smallest level within eps, as a class
-  // 0..4, and the misplaced flux shares of levels 1, 2, 4, 8 ([n][4]).
+  // 0..4, and the deposit errors of levels 1, 2, 4, 8 ([n][4]).
   bool labels(const std::vector<int>& tiles, std::vector<int>& lab, std::vector<float>& err) {
     lab.assign(tiles.size(), 0);
     err.assign(tiles.size() * 4, 0.f);
@@ -127,7 +128,8 @@ class AdaptiveIPM {
   DevVec<int> d_cls_, d_level_, d_list_;
   DevVec<double2> d_ref_;
   DevVec<DepositPiece<float>> d_pieces_;
-  DevVec<unsigned long long> d_acc_, d_diff_;
+  DevVec<int4> d_win_;
+  DevVec<unsigned long long> d_acc_, d_diff_, d_wacc_, d_wdiff_;
   DevVec<T> d_map_;
 
   void setup_geometry() {
@@ -192,7 +194,8 @@ class AdaptiveIPM {
       IRSB_CKR(cudaMemcpyAsync(d_sig_.p, net_sig.data(), kMlpIn * sizeof(float), cudaMemcpyHostToDevice, s));
       mlp_to_bf16<<<ceil_div(kMlpParams, 256), 256, 0, s>>>(d_wf_.p, d_w_.p);
       mlp_classify<<<std::max(1, std::min(ceil_div(nt, 128), 148 * 4)), 128, 0, s>>>(d_w_.p, d_mu_.p, d_sig_.p,
-                                                                                     d_feat_.p, nt, d_cls_.p);
+                                                                                     d_feat_.p, nt, net_quantile,
+                                                                                     d_cls_.p);
       IRSB_LAUNCH_CK("mlp_classify");
       std::vector<int> cls(nt);
       IRSB_CKR(cudaMemcpyAsync(cls.data(), d_cls_.p, nt * sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -208,15 +211,22 @@ class AdaptiveIPM {
     return true;
   }
 
-  // Level-16 interpolation errors of levels 1..8 for isolated tiles.
+  // Deposit errors of levels 1..8 against level 16 for isolated tiles
+  // (ada_window_errors), [tiles][4].
   bool fine_errors(const std::vector<int>& tiles, std::vector<float>& err) {
+    if (tiles.empty()) return true;
     cudaStream_t s = base.stream_;
+    const Params<T>& p = base.prm;
+    const float factor = ipm_triangle_factor<T, float>(p);
     const long long per = 513LL * 513;
-    const int chunk = int(std::max<long long>(1, buffer_cap() / per));
-    if (!d_ref_.alloc_exact(std::min<long long>((long long)chunk, (long long)tiles.size()) * per + 1) ||
-        !d_list_.alloc_exact(std::max<size_t>(tiles.size(), 1)) || !d_err_.alloc_exact(tiles.size() * 4 + 4))
+    const int chunk = int(std::max<long long>(1, std::min<long long>(64, buffer_cap() / per)));
+    const int nc = int(std::min<size_t>(chunk, tiles.size()));
+    if (!d_ref_.alloc_exact(nc * per) || !d_list_.alloc_exact(tiles.size()) || !d_err_.alloc_exact(tiles.size() * 4) ||
+        !d_win_.alloc_exact(nc) || !d_pieces_.alloc_exact(nc * 5))
       return false;
     IRSB_CKR(cudaMemcpyAsync(d_list_.p, tiles.data(), tiles.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    std::vector<int4> win(nc);
+    std::vector<DepositPiece<float>> pieces;
     for (size_t k0 = 0; k0 < tiles.size(); k0 += chunk) {
       const int n = int(std::min<size_t>(chunk, tiles.size() - k0));
       const long long total = per * n;
@@ -227,9 +237,55 @@ class AdaptiveIPM {
       else
         ada_refine_corners<T, false><<<grid, 256, 0, s>>>(g_, sp_, base.leaf_ptrs(), descent(), base.d_verts_.p,
                                                           nullptr, d_list_.p + k0, n, kAdaMaxLevel, per, d_ref_.p);
-      ada_level_errors<<<std::min(n, 148 * 8), 256, 0, s>>>(g_, d_list_.p + k0, n, per, d_ref_.p,
+      ada_tile_windows<<<std::min(n, 148 * 8), 256, 0, s>>>(g_, d_list_.p + k0, n, per, d_ref_.p, d_win_.p);
+      IRSB_LAUNCH_CK("ada windows");
+      IRSB_CKR(cudaMemcpyAsync(win.data(), d_win_.p, n * sizeof(int4), cudaMemcpyDeviceToHost, s));
+      IRSB_CKR(cudaStreamSynchronize(s));
+      // window side of this chunk: the small one unless a tile needs more
+      int ws = kAdaWindow;
+      for (int k = 0; k < n; k++)
+        if (win[k].z > kAdaWindow || win[k].w > kAdaWindow) ws = kAdaWindowLarge;
+      const long long W2 = (long long)ws * ws, WD = (long long)ws * (ws + 1);
+      if (!d_wacc_.alloc_exact(n * 5 * W2) || !d_wdiff_.alloc_exact(n * 5 * WD)) return false;
+      pieces.clear();
+      long long nchunks = 0;
+      for (int k = 0; k < n; k++) {
+        if (win[k].z <= 0) continue;
+        const int t = tiles[k0 + k];
+        const int cx = tile_cells_x(t), cy = tile_cells_y(t);
+        for (int c = 0; c < kAdaLevels; c++) {
+          const int sl = ada_level_of(c);
+          DepositPiece<float> pc;
+          pc.voff = (long long)k * per;
+          pc.vstride = (long long)cx * kAdaMaxLevel + 1;
+          pc.vstep = kAdaMaxLevel / sl;
+          pc.ox = win[k].x;
+          pc.oy = win[k].y;
+          pc.ncx = (long long)cx * sl;
+          pc.ncy = (long long)cy * sl;
+          pc.chunk0 = nchunks;
+          pc.factor = factor / float(sl * sl);
+          pc.r = k * kAdaLevels + c;
+          pieces.push_back(pc);
+          nchunks += (pc.ncx * pc.ncy + 31) / 32;
+        }
+      }
+      IRSB_CKR(cudaMemsetAsync(d_wacc_.p, 0, n * 5 * W2 * sizeof(unsigned long long), s));
+      IRSB_CKR(cudaMemsetAsync(d_wdiff_.p, 0, n * 5 * WD * sizeof(unsigned long long), s));
+      const DepositMaps M{d_wacc_.p, d_wdiff_.p};
+      if (!pieces.empty()) {
+        IRSB_CKR(cudaMemcpyAsync(d_pieces_.p, pieces.data(), pieces.size() * sizeof(DepositPiece<float>),
+                                 cudaMemcpyHostToDevice, s));
+        const int gd = int(std::max<long long>(1, std::min<long long>(ceil_div(nchunks, 8), 148LL * 32)));
+        ipm_deposit_batch<float><<<gd, 256, 0, s>>>(d_ref_.p, d_pieces_.p, int(pieces.size()), nchunks, ws, ws, M,
+                                                    W2, WD);
+        const int gr = std::max(1, std::min(ceil_div((long long)ws * 5 * n * 32, 256), 148 * 8));
+        ipm_resolve_rows<<<gr, 256, 0, s>>>(ws, ws * 5 * n, M);
+      }
+      ada_window_errors<<<std::min(n, 148 * 8), 256, 0, s>>>(g_, d_list_.p + k0, n, ws, factor, d_win_.p, d_wacc_.p,
                                                             d_err_.p + k0 * 4);
-      IRSB_LAUNCH_CK("ada fine errors");
+      IRSB_LAUNCH_CK("ada window errors");
+      IRSB_CKR(cudaStreamSynchronize(s));  // the host pieces are rebuilt for the next chunk
     }
     IRSB_CKR(cudaMemcpyAsync(err.data(), d_err_.p, tiles.size() * 4 * sizeof(float), cudaMemcpyDeviceToHost, s));
     IRSB_CKR(cudaStreamSynchronize(s));
@@ -308,6 +364,8 @@ class AdaptiveIPM {
             pc.voff = (long long)k * per;
             pc.vstride = (long long)cx * sl + 1;
           }
+          pc.vstep = 1;
+          pc.ox = pc.oy = 0.0;
           pc.ncx = (long long)cx * sl;
           pc.ncy = (long long)cy * sl;
           pc.chunk0 = L.nchunks;
@@ -460,7 +518,7 @@ class MlpTrainer {
     IRSB_CKR(cudaMemcpyAsync(b.sig.p, sig, kMlpIn * sizeof(float), cudaMemcpyHostToDevice, s));
     mlp_to_bf16<<<ceil_div(kMlpParams, 256), 256, 0, s>>>(b.w.p, b.wb.p);
     mlp_classify<<<std::max(1, std::min(ceil_div(n, 128), 148 * 4)), 128, 0, s>>>(b.wb.p, b.mu.p, b.sig.p, b.feat.p,
-                                                                                  n, b.lab.p);
+                                                                                  n, 0.f, b.lab.p);
     IRSB_LAUNCH_CK("mlp_classify");
     IRSB_CKR(cudaMemcpyAsync(cls, b.lab.p, n * sizeof(int), cudaMemcpyDeviceToHost, s));
     IRSB_CKR(cudaStreamSynchronize(s));

@@ -459,6 +459,8 @@ class BatchMaker {
         DepositPiece<float> pc;
         pc.voff = used;
         pc.vstride = ncx + 1;
+        pc.vstep = 1;
+        pc.ox = pc.oy = 0.0;
         pc.ncx = ncx;
         pc.ncy = take;
         pc.chunk0 = pp.nchunks;

@@ -99,6 +99,12 @@ int get_expansion_order(Obj* self) { return self->prm.expansion_order; }
 
 // 0: default form (FP32 for float libraries, FP64 for double ones), 1: FP64, 2: FP32
 void set_precision(Obj* self, int mode) { self->precision = mode; }
+void set_shoot_launch(Obj* self, int threads, int ctas_per_sm) {
+  self->shoot_threads = (threads == 128 || threads == 512) ? threads : 256;
+  self->shoot_ctas_per_sm = ctas_per_sm > 0 ? ctas_per_sm : 8;
+}
+int get_shoot_threads(Obj* self) { return self->shoot_threads; }
+int get_shoot_ctas_per_sm(Obj* self) { return self->shoot_ctas_per_sm; }
 int get_precision(Obj* self) { return self->precision; }
 
 // Star field from host memory: n records of (x1, x2, mass), with the field
@@ -381,7 +387,8 @@ void ada_set_policy(void* a, int policy, int uniform_level) {
 void ada_set_levels(void* a, const int* levels, int n) {
   static_cast<Ada*>(a)->given_levels.assign(levels, levels + n);
 }
-void ada_set_tolerance(void* a, double eps_px) { static_cast<Ada*>(a)->eps = eps_px; }
+void ada_set_tolerance(void* a, double eps) { static_cast<Ada*>(a)->eps = eps; }
+void ada_set_quantile(void* a, float q) { static_cast<Ada*>(a)->net_quantile = q; }
 void ada_set_audit(void* a, double fraction, unsigned seed) {
   static_cast<Ada*>(a)->audit_fraction = fraction;
   static_cast<Ada*>(a)->audit_seed = seed;

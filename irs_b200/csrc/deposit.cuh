@@ -319,16 +319,21 @@ template <typename D>
 __device__ __forceinline__ void deposit_warp_cells(const double2* __restrict__ verts, long long ncx, long long vx,
                                                    long long ncells, long long base, D factor, int npx, int npy,
                                                    const DepositMaps& m_total, const DepositMaps& m_min,
-                                                   const DepositMaps& m_sad, int parities) {
+                                                   const DepositMaps& m_sad, int parities, long long vstep = 1,
+                                                   double ox = 0.0, double oy = 0.0) {
   const int lane = threadIdx.x & 31;
   const long long c = base + lane;
   double2 y0 = make_double2(0, 0), y1 = y0, y2 = y0, y3 = y0;
   if (c < ncells) {
     long long j = c / ncx, i = c - j * ncx;
-    y0 = verts[(j + 1) * vx + (i + 1)];  // z + rhs
-    y1 = verts[(j + 1) * vx + i];        // z - conj(rhs)
-    y2 = verts[j * vx + i];              // z - rhs
-    y3 = verts[j * vx + (i + 1)];        // z + conj(rhs)
+    y0 = verts[((j + 1) * vx + (i + 1)) * vstep];  // z + rhs
+    y1 = verts[((j + 1) * vx + i) * vstep];        // z - conj(rhs)
+    y2 = verts[(j * vx + i) * vstep];              // z - rhs
+    y3 = verts[(j * vx + (i + 1)) * vstep];        // z + conj(rhs)
+    if (ox != 0.0 || oy != 0.0) {  // origin of the piece's map in the positions' pixel frame
+      y0.x -= ox, y1.x -= ox, y2.x -= ox, y3.x -= ox;
+      y0.y -= oy, y1.y -= oy, y2.y -= oy, y3.y -= oy;
+    }
   }
 #pragma unroll 1
   for (int half = 0; half < 2; half++) {
@@ -408,6 +413,8 @@ template <typename D>
 struct DepositPiece {
   long long voff;
   long long vstride;   // corner row stride (ncx + 1 for a whole lattice row)
+  long long vstep;     // corner (i, j) is at (j * vstride + i) * vstep (a coarser view of a finer grid)
+  double ox, oy;       // origin of the piece's map in the positions' pixel frame
   long long ncx, ncy;  // cells
   long long chunk0;    // first 32-cell chunk of the piece in the pass
   D factor;
@@ -434,7 +441,7 @@ __global__ void __launch_bounds__(256, sizeof(D) == 4 ? 4 : 2)
     const DepositPiece<D> pc = pieces[lo];
     const DepositMaps M{maps.acc + pc.r * map_stride, maps.diff + pc.r * diff_stride};
     deposit_warp_cells<D>(verts + pc.voff, pc.ncx, pc.vstride, pc.ncx * pc.ncy, (g - pc.chunk0) * 32, pc.factor,
-                          npx, npy, M, M, M, 0);
+                          npx, npy, M, M, M, 0, pc.vstep, pc.ox, pc.oy);
   }
 }
 

@@ -126,6 +126,11 @@ class MapMaker {
   // IPM: stop after the corner lattice (no deposition, no maps); used by the
   // adaptive deposition, which deposits the lattice itself
   bool verts_only = false;
+  // launch shape of the FP32 lens-equation kernel (set by the autotuner):
+  // threads per CTA (128, 256 or 512: 8, 4 or 2 lattice points per thread)
+  // and resident CTAs per SM of its persistent grid
+  int shoot_threads = 256;
+  int shoot_ctas_per_sm = 8;
 
   MapMaker() {
     if (IS_IRS) {
@@ -506,9 +511,24 @@ class MapMaker {
     return lp;
   }
 
-  static int shoot_grid(long long tiles) {
-    long long g = std::min<long long>(tiles, 148LL * 8);
+  int shoot_grid(long long tiles) const {
+    long long g = std::min<long long>(tiles, 148LL * std::max(1, shoot_ctas_per_sm));
     return int(std::max<long long>(g, 1));
+  }
+
+  template <bool VERT, bool PAR, bool GEN>
+  void launch_f32(int grid, const ShootParams& sp, const LeafPtrs& lp, int* pix, int* pmin, int* psad,
+                  double2* verts) {
+    switch (shoot_threads) {
+      case 128:
+        shoot_f32<VERT, PAR, GEN, 128><<<grid, 128, 0, stream_>>>(sp, lp, tiles_.total, pix, pmin, psad, verts);
+        break;
+      case 512:
+        shoot_f32<VERT, PAR, GEN, 512><<<grid, 512, 0, stream_>>>(sp, lp, tiles_.total, pix, pmin, psad, verts);
+        break;
+      default:
+        shoot_f32<VERT, PAR, GEN, 256><<<grid, 256, 0, stream_>>>(sp, lp, tiles_.total, pix, pmin, psad, verts);
+    }
   }
 
   template <bool VERT>
@@ -526,14 +546,14 @@ class MapMaker {
     if (use_fp32()) {
       if (par) {
         if (generic)
-          shoot_f32<VERT, true, true><<<grid, kShootThreads, 0, stream_>>>(sp, lp, tiles_.total, pix, pmin, psad, verts);
+          launch_f32<VERT, true, true>(grid, sp, lp, pix, pmin, psad, verts);
         else
-          shoot_f32<VERT, true, false><<<grid, kShootThreads, 0, stream_>>>(sp, lp, tiles_.total, pix, pmin, psad, verts);
+          launch_f32<VERT, true, false>(grid, sp, lp, pix, pmin, psad, verts);
       } else {
         if (generic)
-          shoot_f32<VERT, false, true><<<grid, kShootThreads, 0, stream_>>>(sp, lp, tiles_.total, pix, pmin, psad, verts);
+          launch_f32<VERT, false, true>(grid, sp, lp, pix, pmin, psad, verts);
         else
-          shoot_f32<VERT, false, false><<<grid, kShootThreads, 0, stream_>>>(sp, lp, tiles_.total, pix, pmin, psad, verts);
+          launch_f32<VERT, false, false>(grid, sp, lp, pix, pmin, psad, verts);
       }
     } else {
       if (par)

@@ -62,10 +62,12 @@ __device__ __forceinline__ void mlp_logits(const float* sw, const float* x, floa
   }
 }
 
-// Level class (argmax of the logits) of each sample.
+// Level class of each sample: the argmax of the logits (q <= 0), or the
+// smallest class whose cumulative softmax probability reaches q (the classes
+// are ordered levels; q > 0.5 leans towards refining).
 __global__ void __launch_bounds__(128) mlp_classify(const __nv_bfloat16* __restrict__ w, const float* __restrict__ mu,
                                                     const float* __restrict__ sig, const float* __restrict__ feat,
-                                                    int n, int* __restrict__ cls) {
+                                                    int n, float q, int* __restrict__ cls) {
   __shared__ float sw[kMlpParams];
   mlp_stage(w, sw);
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
@@ -76,6 +78,23 @@ __global__ void __launch_bounds__(128) mlp_classify(const __nv_bfloat16* __restr
 #pragma unroll
     for (int k = 1; k < kMlpOut; k++)
       if (z3[k] > z3[best]) best = k;
+    if (q > 0.f) {
+      float e[kMlpOut], se = 0.f;
+#pragma unroll
+      for (int k = 0; k < kMlpOut; k++) {
+        e[k] = expf(z3[k] - z3[best]);
+        se += e[k];
+      }
+      float cum = 0.f;
+      best = kMlpOut - 1;
+      for (int k = 0; k < kMlpOut; k++) {
+        cum += e[k] / se;
+        if (cum >= q) {
+          best = k;
+          break;
+        }
+      }
+    }
     cls[s] = best;
   }
 }

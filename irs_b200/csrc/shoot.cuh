@@ -215,11 +215,12 @@ __global__ void __launch_bounds__(kShootThreads) shoot_f64(ShootParams sp, LeafP
 // GENERIC_SMOOTH: the smooth sheet is not the circular approximation
 // (alpha_smooth = -kappa_star z); its deviation from that linear form is then
 // added per point in FP64.
-template <bool VERT, bool PAR, bool GENERIC_SMOOTH>
+template <bool VERT, bool PAR, bool GENERIC_SMOOTH, int THREADS = kShootThreads>
 __device__ __forceinline__ void shoot_f32_tile(const ShootParams& sp, const LeafPtrs& lp, const TileInfo& ti,
                                                const ShootOut& o, float4* s_near, float2* s_coef) {
-  constexpr int R = kRaysPerThread;
-  constexpr int RS = kShootThreads / kTileX;  // row stride between a thread's points
+  static_assert(THREADS >= 128 && THREADS <= 1024 && kTileY % (THREADS / kTileX) == 0, "tile shape");
+  constexpr int R = kTileY / (THREADS / kTileX);  // lattice points per thread
+  constexpr int RS = THREADS / kTileX;            // row stride between a thread's points
   const int tx = threadIdx.x & (kTileX - 1), ty = threadIdx.x / kTileX;
   const cplx<double> corner = mk(sp.corner_re, sp.corner_im);
   // linear part of the lens equation for the circular approximation
@@ -362,15 +363,17 @@ __device__ __forceinline__ void shoot_f32_tile(const ShootParams& sp, const Leaf
   }
 }
 
-template <bool VERT, bool PAR, bool GENERIC_SMOOTH>
-__global__ void __launch_bounds__(kShootThreads) shoot_f32(ShootParams sp, LeafPtrs lp, long long total_tiles,
-                                                           int* __restrict__ pix, int* __restrict__ pmin,
-                                                           int* __restrict__ psad, double2* __restrict__ verts) {
+// THREADS per CTA sets the lattice points per thread, kTileY / (THREADS / 32):
+// 8 at 128 threads, 4 at 256, 2 at 512 (a choice of the autotuner).
+template <bool VERT, bool PAR, bool GENERIC_SMOOTH, int THREADS = kShootThreads>
+__global__ void __launch_bounds__(THREADS) shoot_f32(ShootParams sp, LeafPtrs lp, long long total_tiles,
+                                                     int* __restrict__ pix, int* __restrict__ pmin,
+                                                     int* __restrict__ psad, double2* __restrict__ verts) {
   __shared__ float4 s_near[kMaxStarsDirect];
   __shared__ float2 s_coef[kMaxOrder];
   const ShootOut o{pix, pmin, psad, verts, sp.jbase};
   for (long long t = blockIdx.x; t < total_tiles; t += gridDim.x)
-    shoot_f32_tile<VERT, PAR, GENERIC_SMOOTH>(sp, lp, tile_info(lp, t), o, s_near, s_coef);
+    shoot_f32_tile<VERT, PAR, GENERIC_SMOOTH, THREADS>(sp, lp, tile_info(lp, t), o, s_near, s_coef);
 }
 
 // Many realizations in one launch: the tiles of all their leaves form one work
