@@ -466,6 +466,17 @@ def our_arm(args):
                           "ms_per_step": float(np.mean(ts)) * 1e3, "shoot_ms": r.value("t_lattice") * 1e3,
                           "rays_received": int(r.num_rays_received)}
             r.close()
+        # the same workload through the graph-captured pipeline (one realization)
+        import irs_b200
+        w = {k: v for k, v in WORKLOAD.items() if k not in ("name", "expansion_order")}
+        gb = irs_b200.BatchIPM([{**w, "theta_star": m.theta_star}], expansion_order=p)
+        gb.run()
+        tg = [gb.rerun(1) for _ in range(max(3, args.steps))]
+        extra["ipm_graph_single"] = {"pixels_per_s": npix / float(np.median(tg)),
+                                     "ms_per_step": float(np.median(tg)) * 1e3,
+                                     "graph_nodes": int(gb.value("graph_nodes")),
+                                     "map_equals_headline": bool(np.array_equal(gb.maps[0], m.magnifications))}
+        gb.close()
         extra["batched_256"] = batch_measure(args.steps)
         extra["learned_adaptive"] = adaptive_measure()
 

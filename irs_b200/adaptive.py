@@ -88,14 +88,16 @@ class AdaptiveIPM:
     """An IPM map with per-tile subdivision.
 
     policy: "network" (levels from `network`), "uniform" (every tile at
-    `level`) or "given" (per-tile `levels`). tolerance: share of a tile's flux
-    that its level may put in other pixels than level 16 does (labels and
-    audit). quantile: a tile takes the smallest level whose cumulative network
+    `level`) or "given" (per-tile `levels`). tolerance: the deposit error a
+    tile's level may make against level 16 (labels and audit): a share of the
+    tile's own flux (error_mode 0) or of the map's flux where the tile lands
+    (error_mode 1). quantile: a tile takes the smallest level whose cumulative network
     probability reaches it (above 0.5 leans towards refining). The map inputs
     are those of IPM (keyword arguments)."""
 
-    def __init__(self, network=None, policy="network", level=1, levels=None, tolerance=1e-3,
-                 audit_fraction=0.01, audit_seed=1, refine_capacity=0, quantile=0.8, is_double=False, verbose=0,
+    def __init__(self, network=None, policy="network", level=1, levels=None, tolerance=5e-4,
+                 audit_fraction=0.01, audit_seed=1, refine_capacity=0, quantile=0.8, error_mode=0, is_double=False,
+                 verbose=0,
                  **ipm_kwargs):
         self.is_double = bool(is_double)
         self.lib = _lib.load("ipm", self.is_double)
@@ -115,6 +117,7 @@ class AdaptiveIPM:
             self.lib.ada_set_levels(self.h, _fp(lv), len(lv))
         self.lib.ada_set_tolerance(self.h, float(tolerance))
         self.lib.ada_set_quantile(self.h, float(quantile))
+        self.lib.ada_set_error_mode(self.h, int(error_mode))
         self.lib.ada_set_audit(self.h, float(audit_fraction), int(audit_seed))
         self.lib.ada_set_refine_capacity(self.h, int(refine_capacity))
 

@@ -23,10 +23,10 @@
 //     identically.
 //
 // Labels for training: a tile's label is the smallest level s whose deposit
-// differs from the tile's level-16 deposit by at most a share eps of its flux
-// (relative L1 over the tile's own pixel window; 16 when no coarser level
-// does): the level at which the tile's deposit converges to the uniform-fine
-// map.
+// differs from the tile's level-16 deposit by at most eps (ada_window_errors:
+// a share of the tile's own flux, or of the map's flux where it lands), 16
+// when no coarser level does: the level at which the tile's deposit
+// converges to the uniform-fine map.
 #pragma once
 #include "deposit.cuh"
 #include "leaves.cuh"
@@ -219,16 +219,17 @@ __global__ void __launch_bounds__(256) ada_refine_corners(AdaGeom g, ShootParams
 // Deposit error of levels 1, 2, 4, 8 against level 16, tile by tile. Each
 // tile is deposited on its own into a private pixel window at every level
 // (level-s corners are every (16/s)-th level-16 corner), and
-//   err[slot * 4 + c] = sum |W_c - W_16| / (2 factor * cells of the tile)
-// over the window, W_c being the tile's deposit at level 2^c: the share of
-// the tile's flux that level 2^c puts in the wrong pixels.
+//   err[slot * 4 + c] = sum |W_c - W_16| / reference flux
+// over the map pixels in the window, W_c being the tile's deposit at level 2^c
+// (the reference is below).
 constexpr int kAdaWindow = 256;       // pixels per side of a tile's window
 constexpr int kAdaWindowLarge = 1024; // window of a chunk holding a tile whose image needs more
 constexpr int kAdaWindowMargin = 2;
 
 // Window of each tile: the pixel bounding box of its level-16 image within the
 // map, widened by kAdaWindowMargin; win[slot] = (x0, y0, w, h), w = 0 when the
-// image misses the map, w = -1 when the box exceeds the large window.
+// image misses the map. A box wider than the chunk's window is covered at a
+// coarser pixel scale (ada_window_scale).
 __global__ void __launch_bounds__(256) ada_tile_windows(AdaGeom g, const int* __restrict__ list, int nlist,
                                                         long long stride, const double2* __restrict__ fine,
                                                         int4* __restrict__ win) {
@@ -271,39 +272,61 @@ __global__ void __launch_bounds__(256) ada_tile_windows(AdaGeom g, const int* __
       const double x1 = fmin(ceil(r[2]) + kAdaWindowMargin, double(g.npx));
       const double y1 = fmin(ceil(r[3]) + kAdaWindowMargin, double(g.npy));
       int4 o = make_int4(0, 0, 0, 0);
-      if (x1 > x0 && y1 > y0) {
-        o = make_int4(int(x0), int(y0), int(x1 - x0), int(y1 - y0));
-        if (o.z > kAdaWindowLarge || o.w > kAdaWindowLarge) o.z = -1;
-      }
+      if (x1 > x0 && y1 > y0) o = make_int4(int(x0), int(y0), int(x1 - x0), int(y1 - y0));
       win[slot] = o;
     }
     __syncthreads();
   }
 }
 
+// Map pixels per window pixel for a tile's window (1 unless its image is
+// wider than the window side ws).
+__host__ __device__ __forceinline__ int ada_window_scale(int4 w, int ws) {
+  const int m = w.z > w.w ? w.z : w.w;
+  return m <= ws ? 1 : (m + ws - 1) / ws;
+}
+
 // Differences of the resolved windows of side ws (window of slot k, level c
-// at acc + (k * 5 + c) * ws^2) as a share of the tile's whole flux (2 factor
-// per cell, on the map or not), so that a tile with little flux on the map
-// cannot have a large error.
+// at acc + (k * 5 + c) * ws^2, placed at (win.x, win.y) on the map): the flux
+// the tile puts in other map pixels at level 2^c than at level 16, as a share
+// of
+//   mode 0: the tile's whole flux (2 factor per cell): its own relative error,
+//           which the map inherits where the errors of overlapping tiles have
+//           the same sign (the bias of the triangle approximation);
+//   mode 1: the flux of the plain (level 1) map `ref` in the pixels the tile
+//           reaches (at least the tile's own level-16 flux): its share of the
+//           map's relative error there when the errors of overlapping tiles
+//           are independent.
 __global__ void __launch_bounds__(256) ada_window_errors(AdaGeom g, const int* __restrict__ list, int nlist, int ws,
-                                                         float factor, const int4* __restrict__ win,
+                                                         float factor, int mode, const int4* __restrict__ win,
                                                          const unsigned long long* __restrict__ acc,
+                                                         const unsigned long long* __restrict__ ref,
                                                          float* __restrict__ err) {
   __shared__ double red[5][8];
   const long long W2 = (long long)ws * ws;
   for (int slot = blockIdx.x; slot < nlist; slot += gridDim.x) {
     const int4 w = win[slot];
     if (w.z <= 0) {  // uniform over the block
-      if (threadIdx.x < 4) err[(long long)slot * 4 + threadIdx.x] = w.z < 0 ? 1.f : 0.f;
+      if (threadIdx.x < 4) err[(long long)slot * 4 + threadIdx.x] = 0.f;
       continue;
     }
+    const int k = ada_window_scale(w, ws);
     const unsigned long long* A = acc + (long long)slot * 5 * W2;
     double d[4] = {0, 0, 0, 0}, tot = 0;
     for (long long q = threadIdx.x; q < W2; q += blockDim.x) {
+      const int x = w.x + int(q % ws) * k, y = w.y + int(q / ws) * k;
+      if (x >= g.npx || y >= g.npy) continue;  // the window runs past the map's edge
       const long long a16 = (long long)A[4 * W2 + q];
-      tot += double(a16);
+      bool touched = a16 != 0;
 #pragma unroll
-      for (int c = 0; c < 4; c++) d[c] += fabs(double((long long)A[c * W2 + q] - a16));
+      for (int c = 0; c < 4; c++) {
+        const long long ac = (long long)A[c * W2 + q];
+        touched = touched || ac != 0;
+        d[c] += fabs(double(ac - a16));
+      }
+      // where the plain map holds less than the tile's own flux, the tile's
+      // flux is the reference
+      if (touched && mode == 1) tot += fmax(double(ref[(long long)y * g.npx + x]), double(a16));
     }
 #pragma unroll
     for (int c = 0; c < 5; c++) {
@@ -313,13 +336,18 @@ __global__ void __launch_bounds__(256) ada_window_errors(AdaGeom g, const int* _
     }
     __syncthreads();
     if (threadIdx.x < 4) {
-      const int t = list[slot];
-      const long long cells = llmin_(kAdaTile, g.ncx - (long long)(t % g.ntx) * kAdaTile) *
-                              llmin_(kAdaTile, g.ncy - (long long)(t / g.ntx) * kAdaTile);
-      const double whole = double(cells) * 2.0 * double(factor) * kFixScale;
-      double num = 0;
-      for (int k = 0; k < int(blockDim.x >> 5); k++) num += red[threadIdx.x][k];
-      err[(long long)slot * 4 + threadIdx.x] = float(num / whole);
+      double num = 0, den = 0;
+      for (int k = 0; k < int(blockDim.x >> 5); k++) {
+        num += red[threadIdx.x][k];
+        den += red[4][k];
+      }
+      if (mode == 0) {
+        const int t = list[slot];
+        const long long cells = llmin_(kAdaTile, g.ncx - (long long)(t % g.ntx) * kAdaTile) *
+                                llmin_(kAdaTile, g.ncy - (long long)(t / g.ntx) * kAdaTile);
+        den = double(cells) * 2.0 * double(factor) * kFixScale;
+      }
+      err[(long long)slot * 4 + threadIdx.x] = den > 0 ? float(num / den) : (num > 0 ? 1.f : 0.f);
     }
     __syncthreads();
   }

@@ -34,7 +34,8 @@ class AdaptiveIPM {
   int policy = kAdaNetwork;
   int uniform_level = 1;
   std::vector<int> given_levels;
-  double eps = 1e-3;             // tolerance: share of a tile's flux its level may put in wrong pixels
+  double eps = 5e-4;             // tolerance of a tile's deposit error (err_mode)
+  int err_mode = 0;              // 0: share of the tile's own flux; 1: share of the map's flux where it lands
   double audit_fraction = 0.01;  // share of tiles audited per run
   unsigned audit_seed = 1;
   long long refine_cap = 0;      // corner positions in the refinement buffer (0: automatic)
@@ -66,6 +67,7 @@ class AdaptiveIPM {
       IRSB_CKR(cudaEventCreate(&e1_));
     }
     setup_geometry();
+    base_map_ready_ = false;
     IRSB_CKR(cudaEventRecord(e0_, s));
     if (!features()) return false;
     if (!choose_levels()) return false;
@@ -129,7 +131,8 @@ class AdaptiveIPM {
   DevVec<double2> d_ref_;
   DevVec<DepositPiece<float>> d_pieces_;
   DevVec<int4> d_win_;
-  DevVec<unsigned long long> d_acc_, d_diff_, d_wacc_, d_wdiff_;
+  DevVec<unsigned long long> d_acc_, d_diff_, d_wacc_, d_wdiff_, d_bacc_, d_bdiff_;
+  bool base_map_ready_ = false;
   DevVec<T> d_map_;
 
   void setup_geometry() {
@@ -218,6 +221,7 @@ class AdaptiveIPM {
     cudaStream_t s = base.stream_;
     const Params<T>& p = base.prm;
     const float factor = ipm_triangle_factor<T, float>(p);
+    if (err_mode == 1 && !base_map_ready_ && !base_map()) return false;
     const long long per = 513LL * 513;
     const int chunk = int(std::max<long long>(1, std::min<long long>(64, buffer_cap() / per)));
     const int nc = int(std::min<size_t>(chunk, tiles.size()));
@@ -261,6 +265,7 @@ class AdaptiveIPM {
           pc.vstep = kAdaMaxLevel / sl;
           pc.ox = win[k].x;
           pc.oy = win[k].y;
+          pc.inv_scale = 1.0 / ada_window_scale(win[k], ws);
           pc.ncx = (long long)cx * sl;
           pc.ncy = (long long)cy * sl;
           pc.chunk0 = nchunks;
@@ -282,13 +287,34 @@ class AdaptiveIPM {
         const int gr = std::max(1, std::min(ceil_div((long long)ws * 5 * n * 32, 256), 148 * 8));
         ipm_resolve_rows<<<gr, 256, 0, s>>>(ws, ws * 5 * n, M);
       }
-      ada_window_errors<<<std::min(n, 148 * 8), 256, 0, s>>>(g_, d_list_.p + k0, n, ws, factor, d_win_.p, d_wacc_.p,
-                                                            d_err_.p + k0 * 4);
+      ada_window_errors<<<std::min(n, 148 * 8), 256, 0, s>>>(g_, d_list_.p + k0, n, ws, factor, err_mode, d_win_.p,
+                                                            d_wacc_.p, d_bacc_.p, d_err_.p + k0 * 4);
       IRSB_LAUNCH_CK("ada window errors");
       IRSB_CKR(cudaStreamSynchronize(s));  // the host pieces are rebuilt for the next chunk
     }
     IRSB_CKR(cudaMemcpyAsync(err.data(), d_err_.p, tiles.size() * 4 * sizeof(float), cudaMemcpyDeviceToHost, s));
     IRSB_CKR(cudaStreamSynchronize(s));
+    return true;
+  }
+
+  // The plain (level 1) map in fixed point, the reference of the tile errors.
+  bool base_map() {
+    cudaStream_t s = base.stream_;
+    const Params<T>& p = base.prm;
+    const int npx = p.num_pixels_y.re, npy = p.num_pixels_y.im;
+    const long long npix = (long long)npx * npy, ndiff = (long long)npy * (npx + 1);
+    if (!d_bacc_.alloc_exact(npix) || !d_bdiff_.alloc_exact(ndiff)) return false;
+    IRSB_CKR(cudaMemsetAsync(d_bacc_.p, 0, npix * sizeof(unsigned long long), s));
+    IRSB_CKR(cudaMemsetAsync(d_bdiff_.p, 0, ndiff * sizeof(unsigned long long), s));
+    const DepositMaps M{d_bacc_.p, d_bdiff_.p};
+    const long long ncells = g_.ncx * g_.ncy;
+    const int grid = int(std::max<long long>(1, std::min<long long>((ncells + 255) / 256, 148LL * 16)));
+    ipm_deposit_cells<float><<<grid, 256, 0, s>>>(base.d_verts_.p, g_.ncx, g_.ncy, ipm_triangle_factor<T, float>(p),
+                                                  npx, npy, M, M, M, 0);
+    const int gr = std::max(1, std::min(ceil_div((long long)npy * 32, 256), 148 * 8));
+    ipm_resolve_rows<<<gr, 256, 0, s>>>(npx, npy, M);
+    IRSB_LAUNCH_CK("ada base map");
+    base_map_ready_ = true;
     return true;
   }
 
@@ -366,6 +392,7 @@ class AdaptiveIPM {
           }
           pc.vstep = 1;
           pc.ox = pc.oy = 0.0;
+        pc.inv_scale = 1.0;
           pc.ncx = (long long)cx * sl;
           pc.ncy = (long long)cy * sl;
           pc.chunk0 = L.nchunks;

@@ -461,6 +461,7 @@ class BatchMaker {
         pc.vstride = ncx + 1;
         pc.vstep = 1;
         pc.ox = pc.oy = 0.0;
+        pc.inv_scale = 1.0;
         pc.ncx = ncx;
         pc.ncy = take;
         pc.chunk0 = pp.nchunks;

@@ -320,7 +320,7 @@ __device__ __forceinline__ void deposit_warp_cells(const double2* __restrict__ v
                                                    long long ncells, long long base, D factor, int npx, int npy,
                                                    const DepositMaps& m_total, const DepositMaps& m_min,
                                                    const DepositMaps& m_sad, int parities, long long vstep = 1,
-                                                   double ox = 0.0, double oy = 0.0) {
+                                                   double ox = 0.0, double oy = 0.0, double inv_scale = 1.0) {
   const int lane = threadIdx.x & 31;
   const long long c = base + lane;
   double2 y0 = make_double2(0, 0), y1 = y0, y2 = y0, y3 = y0;
@@ -333,6 +333,10 @@ __device__ __forceinline__ void deposit_warp_cells(const double2* __restrict__ v
     if (ox != 0.0 || oy != 0.0) {  // origin of the piece's map in the positions' pixel frame
       y0.x -= ox, y1.x -= ox, y2.x -= ox, y3.x -= ox;
       y0.y -= oy, y1.y -= oy, y2.y -= oy, y3.y -= oy;
+    }
+    if (inv_scale != 1.0) {  // the piece's map has pixels 1 / inv_scale wide
+      y0.x *= inv_scale, y1.x *= inv_scale, y2.x *= inv_scale, y3.x *= inv_scale;
+      y0.y *= inv_scale, y1.y *= inv_scale, y2.y *= inv_scale, y3.y *= inv_scale;
     }
   }
 #pragma unroll 1
@@ -415,6 +419,7 @@ struct DepositPiece {
   long long vstride;   // corner row stride (ncx + 1 for a whole lattice row)
   long long vstep;     // corner (i, j) is at (j * vstride + i) * vstep (a coarser view of a finer grid)
   double ox, oy;       // origin of the piece's map in the positions' pixel frame
+  double inv_scale;    // 1 / width of the piece's map pixels in the positions' pixels
   long long ncx, ncy;  // cells
   long long chunk0;    // first 32-cell chunk of the piece in the pass
   D factor;
@@ -441,7 +446,7 @@ __global__ void __launch_bounds__(256, sizeof(D) == 4 ? 4 : 2)
     const DepositPiece<D> pc = pieces[lo];
     const DepositMaps M{maps.acc + pc.r * map_stride, maps.diff + pc.r * diff_stride};
     deposit_warp_cells<D>(verts + pc.voff, pc.ncx, pc.vstride, pc.ncx * pc.ncy, (g - pc.chunk0) * 32, pc.factor,
-                          npx, npy, M, M, M, 0, pc.vstep, pc.ox, pc.oy);
+                          npx, npy, M, M, M, 0, pc.vstep, pc.ox, pc.oy, pc.inv_scale);
   }
 }
 

@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 ADA = dict(kappa_tot=0.45, shear=0.4, smooth_fraction=0.5, mass_function="salpeter", m_lower=0.08, m_upper=1.0,
            theta_star=1.0, half_length_y1=4.0, half_length_y2=4.0, num_pixels_y1=128, num_pixels_y2=128,
            random_seed=4, write_histograms=0)
-EPS = 1e-3
+EPS = 5e-4
 
 
 def _ada(**kw):
@@ -148,4 +148,4 @@ def test_network_gain_over_uniform_subdivision(gpu):
     print(f"network error {e_net:.2e}, matching uniform level {match}, gain {gain:.2f}, "
           f"audit {a.value('audit_failures'):.0f}/{a.value('audited'):.0f}")
     assert e_net < 1e-3
-    assert gain > 1.5
+    assert gain > 1.2
