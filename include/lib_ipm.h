@@ -171,7 +171,7 @@ IPMHandle* ada_base(void* ada);                                   /* the map's i
 void ada_set_policy(void* ada, int policy, int uniform_level);    /* 0 network, 1 uniform level, 2 given levels */
 void ada_set_levels(void* ada, const int* levels, int n);         /* policy 2: one level per tile, row-major */
 void ada_set_tolerance(void* ada, double eps);                    /* tolerance of a tile's deposit error */
-void ada_set_error_mode(void* ada, int mode);   /* error as a share of 0: the tile's flux, 1: the map's flux there */
+void ada_set_error_mode(void* ada, int mode);   /* error as a share of 0: the tile's flux, 1: the map's flux there, 2: the smaller */
 void ada_set_quantile(void* ada, float q);                        /* network: smallest level with cumulative p >= q */
 void ada_set_audit(void* ada, double fraction, unsigned seed);
 void ada_set_refine_capacity(void* ada, long long corners);       /* refinement buffer, 0: automatic */

@@ -225,6 +225,7 @@ __global__ void __launch_bounds__(256) ada_refine_corners(AdaGeom g, ShootParams
 constexpr int kAdaWindow = 256;       // pixels per side of a tile's window
 constexpr int kAdaWindowLarge = 1024; // window of a chunk holding a tile whose image needs more
 constexpr int kAdaWindowMargin = 2;
+constexpr double kAdaMapWeight = 20.0;  // mode 2: weight of the map-relative error
 
 // Window of each tile: the pixel bounding box of its level-16 image within the
 // map, widened by kAdaWindowMargin; win[slot] = (x0, y0, w, h), w = 0 when the
@@ -296,7 +297,12 @@ __host__ __device__ __forceinline__ int ada_window_scale(int4 w, int ws) {
 //   mode 1: the flux of the plain (level 1) map `ref` in the pixels the tile
 //           reaches (at least the tile's own level-16 flux): its share of the
 //           map's relative error there when the errors of overlapping tiles
-//           are independent.
+//           are independent;
+//   mode 2: the smaller of the mode-0 error and kAdaMapWeight times the
+//           mode-1 error: a tile passes when its own deposit is accurate or
+//           when its error is a small part of the map where it lands (images
+//           close to a star, stretched thin over pixels that other images
+//           fill).
 __global__ void __launch_bounds__(256) ada_window_errors(AdaGeom g, const int* __restrict__ list, int nlist, int ws,
                                                          float factor, int mode, const int4* __restrict__ win,
                                                          const unsigned long long* __restrict__ acc,
@@ -326,7 +332,7 @@ __global__ void __launch_bounds__(256) ada_window_errors(AdaGeom g, const int* _
       }
       // where the plain map holds less than the tile's own flux, the tile's
       // flux is the reference
-      if (touched && mode == 1) tot += fmax(double(ref[(long long)y * g.npx + x]), double(a16));
+      if (touched && mode >= 1) tot += fmax(double(ref[(long long)y * g.npx + x]), double(a16));
     }
 #pragma unroll
     for (int c = 0; c < 5; c++) {
@@ -341,13 +347,13 @@ __global__ void __launch_bounds__(256) ada_window_errors(AdaGeom g, const int* _
         num += red[threadIdx.x][k];
         den += red[4][k];
       }
-      if (mode == 0) {
-        const int t = list[slot];
-        const long long cells = llmin_(kAdaTile, g.ncx - (long long)(t % g.ntx) * kAdaTile) *
-                                llmin_(kAdaTile, g.ncy - (long long)(t / g.ntx) * kAdaTile);
-        den = double(cells) * 2.0 * double(factor) * kFixScale;
-      }
-      err[(long long)slot * 4 + threadIdx.x] = den > 0 ? float(num / den) : (num > 0 ? 1.f : 0.f);
+      const int t = list[slot];
+      const long long cells = llmin_(kAdaTile, g.ncx - (long long)(t % g.ntx) * kAdaTile) *
+                              llmin_(kAdaTile, g.ncy - (long long)(t / g.ntx) * kAdaTile);
+      const double own = double(cells) * 2.0 * double(factor) * kFixScale;
+      const double e_map = den > 0 ? num / den : (num > 0 ? 1.0 : 0.0);
+      const double e = mode == 0 ? num / own : (mode == 1 ? e_map : fmin(num / own, kAdaMapWeight * e_map));
+      err[(long long)slot * 4 + threadIdx.x] = float(e);
     }
     __syncthreads();
   }

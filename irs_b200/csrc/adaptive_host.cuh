@@ -35,7 +35,7 @@ class AdaptiveIPM {
   int uniform_level = 1;
   std::vector<int> given_levels;
   double eps = 5e-4;             // tolerance of a tile's deposit error (err_mode)
-  int err_mode = 0;              // 0: share of the tile's own flux; 1: share of the map's flux where it lands
+  int err_mode = 0;  // 0: share of the tile's own flux; 1: of the map's flux where it lands; 2: the smaller (ada_window_errors)
   double audit_fraction = 0.01;  // share of tiles audited per run
   unsigned audit_seed = 1;
   long long refine_cap = 0;      // corner positions in the refinement buffer (0: automatic)
@@ -221,7 +221,7 @@ class AdaptiveIPM {
     cudaStream_t s = base.stream_;
     const Params<T>& p = base.prm;
     const float factor = ipm_triangle_factor<T, float>(p);
-    if (err_mode == 1 && !base_map_ready_ && !base_map()) return false;
+    if (err_mode >= 1 && !base_map_ready_ && !base_map()) return false;
     const long long per = 513LL * 513;
     const int chunk = int(std::max<long long>(1, std::min<long long>(64, buffer_cap() / per)));
     const int nc = int(std::min<size_t>(chunk, tiles.size()));
