@@ -290,11 +290,11 @@ ADAPTIVE_CONFIG = dict(kappa_tot=0.6, shear=0.3, smooth_fraction=0.3, mass_funct
 
 def adaptive_measure():
     """The learned-adaptive form on its configuration (4096^2 map): the
-    network-chosen map against the uniform-fine (level 16) map; the uniform
-    level whose map error matches it; and the plain uniform FP64 form at that
-    level (num_rays_y = level^2 cells per pixel area), its tree and
-    expansions timed once and its shooting timed on a band of lattice rows and
-    scaled to the lattice."""
+    network-chosen map against the uniform-fine (level 16) map; the cells a
+    uniform subdivision needs for the same error (interpolated between the
+    uniform levels' errors); and the plain uniform FP64 form at that cost,
+    its tree and expansions timed once and its shooting per cell timed on a
+    band of lattice rows at level 4 (num_rays_y = 16)."""
     import irs_b200
 
     def rel_err(mu, ref):
@@ -321,29 +321,43 @@ def adaptive_measure():
     u16.close()
     med_a, p99_a = rel_err(mu_a, ref)
     res.update({"median_rel_err_vs_uniform16": med_a, "p99_rel_err_vs_uniform16": p99_a})
-    match = 16
     for L in (1, 2, 4, 8):
         u = irs_b200.AdaptiveIPM(policy="uniform", level=L, audit_fraction=0.0, **cfg)
         u.run()
-        med, _ = rel_err(u.magnifications, ref)
-        res[f"uniform{L}_median_rel_err"] = med
+        res[f"uniform{L}_median_rel_err"] = rel_err(u.magnifications, ref)[0]
         u.close()
-        if med <= med_a and match == 16:
-            match = L
-    res["uniform_level_matching_error"] = match
-    p = irs_b200.IPM(**{**cfg, "num_rays_y": match * match}, is_double=True)
+    # cells (in base cells) a uniform subdivision needs for the adaptive map's
+    # error: log-log interpolation of the uniform levels' errors against L^2
+    pts = [(float(L * L), res[f"uniform{L}_median_rel_err"]) for L in (1, 2, 4, 8)]
+    f_match = None
+    if med_a >= pts[0][1]:
+        f_match = 1.0
+    for (f0, e0), (f1, e1) in zip(pts, pts[1:]):
+        if f_match is None and e1 <= med_a <= e0:
+            f_match = f0 * (f1 / f0) ** (np.log(med_a / e0) / np.log(e1 / e0))
+    if f_match is None:  # below level 8: continue the last slope
+        (f0, e0), (f1, e1) = pts[-2], pts[-1]
+        f_match = f1 * (f1 / f0) ** (np.log(med_a / e1) / np.log(e1 / e0))
+    res["uniform_cells_factor_matching_error"] = float(f_match)
+    # plain uniform FP64 at level 4 (num_rays_y = 16) on 1/16 of the rows: its
+    # tree and expansions once, its shooting per cell, scaled to f_match
+    L = 4
+    p = irs_b200.IPM(**{**cfg, "num_rays_y": L * L}, is_double=True)
     p.derive()
     ny = int(p.value("num_ray_threads_2"))
+    nx = int(p.value("num_ray_threads_1"))
     rows = max(1, ny // 16)
     p.lib.set_band(p.obj, 0, rows)
     p.run()
     tb = p.rerun(1)
     shoot = p.value("t_lattice") + p.value("t_deposit")
-    t_plain = (tb - shoot) + shoot * ny / rows  # tree and expansions once, shooting for every row
     p.close()
-    res.update({"plain_fp64_s_at_matching_level": t_plain, "adaptive_s": t_ada,
-                "effective_cells_per_s_adaptive": res["cells_base"] * match * match / t_ada,
-                "effective_cells_per_s_plain_fp64": res["cells_base"] * match * match / t_plain,
+    per_cell = shoot / (float(nx) * rows)
+    t_plain = (tb - shoot) + per_cell * res["cells_base"] * f_match
+    res.update({"plain_fp64_s_at_matching_cells": t_plain, "plain_fp64_ns_per_cell": per_cell * 1e9,
+                "adaptive_s": t_ada,
+                "effective_cells_per_s_adaptive": res["cells_base"] * f_match / t_ada,
+                "effective_cells_per_s_plain_fp64": res["cells_base"] * f_match / t_plain,
                 "adaptive_over_plain_fp64": t_plain / t_ada})
     return res
 

@@ -173,6 +173,7 @@ void ada_set_levels(void* ada, const int* levels, int n);         /* policy 2: o
 void ada_set_tolerance(void* ada, double eps);                    /* tolerance of a tile's deposit error */
 void ada_set_error_mode(void* ada, int mode);   /* error as a share of 0: the tile's flux, 1: the map's flux there, 2: the smaller */
 void ada_set_quantile(void* ada, float q);                        /* network: smallest level with cumulative p >= q */
+void ada_set_max_level(void* ada, int level);                     /* labels / network stop here; the audit may go to 16 */
 void ada_set_audit(void* ada, double fraction, unsigned seed);
 void ada_set_refine_capacity(void* ada, long long corners);       /* refinement buffer, 0: automatic */
 void ada_set_network(void* ada, const float* w, const float* mu, const float* sig); /* 5061 weights, 8 + 8 */

@@ -91,12 +91,14 @@ class AdaptiveIPM:
     `level`) or "given" (per-tile `levels`). tolerance: the deposit error a
     tile's level may make against level 16 (labels and audit): a share of the
     tile's own flux (error_mode 0) or of the map's flux where the tile lands
-    (error_mode 1). quantile: a tile takes the smallest level whose cumulative network
+    (error_mode 1). max_level: the largest level of labels and network
+    choices (tiles near stars would ask for 16 at a large cost and a small
+    gain in the map); the audit still sends a failing tile to 16. quantile: a tile takes the smallest level whose cumulative network
     probability reaches it (above 0.5 leans towards refining). The map inputs
     are those of IPM (keyword arguments)."""
 
-    def __init__(self, network=None, policy="network", level=1, levels=None, tolerance=5e-4,
-                 audit_fraction=0.01, audit_seed=1, refine_capacity=0, quantile=0.8, error_mode=0, is_double=False,
+    def __init__(self, network=None, policy="network", level=1, levels=None, tolerance=1e-4,
+                 audit_fraction=0.01, audit_seed=1, refine_capacity=0, quantile=0.8, error_mode=0, max_level=8, is_double=False,
                  verbose=0,
                  **ipm_kwargs):
         self.is_double = bool(is_double)
@@ -118,6 +120,9 @@ class AdaptiveIPM:
         self.lib.ada_set_tolerance(self.h, float(tolerance))
         self.lib.ada_set_quantile(self.h, float(quantile))
         self.lib.ada_set_error_mode(self.h, int(error_mode))
+        if max_level not in LEVELS:
+            raise ValueError("max_level must be 1, 2, 4, 8 or 16")
+        self.lib.ada_set_max_level(self.h, int(max_level))
         self.lib.ada_set_audit(self.h, float(audit_fraction), int(audit_seed))
         self.lib.ada_set_refine_capacity(self.h, int(refine_capacity))
 

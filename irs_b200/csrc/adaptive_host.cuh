@@ -34,7 +34,8 @@ class AdaptiveIPM {
   int policy = kAdaNetwork;
   int uniform_level = 1;
   std::vector<int> given_levels;
-  double eps = 5e-4;             // tolerance of a tile's deposit error (err_mode)
+  double eps = 1e-4;             // tolerance of a tile's deposit error (err_mode)
+  int max_level = 8;  // labels and network choices stop here; only the audit sends tiles to 16
   int err_mode = 0;  // 0: share of the tile's own flux; 1: of the map's flux where it lands; 2: the smaller (ada_window_errors)
   double audit_fraction = 0.01;  // share of tiles audited per run
   unsigned audit_seed = 1;
@@ -88,12 +89,14 @@ class AdaptiveIPM {
     return true;
   }
 
-  // Labels of `tiles` (after run): smallest level within eps, as a class
-  // 0..4, and the deposit errors of levels 1, 2, 4, 8 ([n][4]).
+  // Labels of `tiles` (after run): smallest level within eps, at most
+  // max_level, as a class 0..4, and the deposit errors of levels 1, 2, 4, 8
+  // ([n][4]).
   bool labels(const std::vector<int>& tiles, std::vector<int>& lab, std::vector<float>& err) {
     lab.assign(tiles.size(), 0);
     err.assign(tiles.size() * 4, 0.f);
     if (!fine_errors(tiles, err)) return false;
+    const int cmax = __builtin_ctz(std::max(1, std::min(kAdaMaxLevel, max_level)));
     for (size_t k = 0; k < tiles.size(); k++) {
       int c = 4;
       for (int q = 0; q < 4; q++)
@@ -101,7 +104,7 @@ class AdaptiveIPM {
           c = q;
           break;
         }
-      lab[k] = c;
+      lab[k] = std::min(c, cmax);
     }
     return true;
   }
@@ -203,7 +206,7 @@ class AdaptiveIPM {
       std::vector<int> cls(nt);
       IRSB_CKR(cudaMemcpyAsync(cls.data(), d_cls_.p, nt * sizeof(int), cudaMemcpyDeviceToHost, s));
       IRSB_CKR(cudaStreamSynchronize(s));
-      for (int t = 0; t < nt; t++) level[t] = ada_level_of(cls[t]);
+      for (int t = 0; t < nt; t++) level[t] = std::min(ada_level_of(cls[t]), std::max(1, max_level));
     }
     for (int v : level)
       if (v != 1 && v != 2 && v != 4 && v != 8 && v != 16) {

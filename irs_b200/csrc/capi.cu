@@ -389,6 +389,7 @@ void ada_set_levels(void* a, const int* levels, int n) {
 }
 void ada_set_tolerance(void* a, double eps) { static_cast<Ada*>(a)->eps = eps; }
 void ada_set_quantile(void* a, float q) { static_cast<Ada*>(a)->net_quantile = q; }
+void ada_set_max_level(void* a, int level) { static_cast<Ada*>(a)->max_level = level; }
 void ada_set_error_mode(void* a, int mode) { static_cast<Ada*>(a)->err_mode = (mode == 1 || mode == 2) ? mode : 0; }
 void ada_set_audit(void* a, double fraction, unsigned seed) {
   static_cast<Ada*>(a)->audit_fraction = fraction;

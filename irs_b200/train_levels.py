@@ -54,7 +54,7 @@ def main():
     ap.add_argument("--first-seed", type=int, default=2000)
     ap.add_argument("--maps", type=int, default=64)
     ap.add_argument("--tiles-per-map", type=int, default=2000)
-    ap.add_argument("--tolerance", type=float, default=5e-4)
+    ap.add_argument("--tolerance", type=float, default=1e-4)
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--batch", type=int, default=512)
     ap.add_argument("--lr", type=float, default=3e-3)

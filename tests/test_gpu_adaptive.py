@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 ADA = dict(kappa_tot=0.45, shear=0.4, smooth_fraction=0.5, mass_function="salpeter", m_lower=0.08, m_upper=1.0,
            theta_star=1.0, half_length_y1=4.0, half_length_y2=4.0, num_pixels_y1=128, num_pixels_y2=128,
            random_seed=4, write_histograms=0)
-EPS = 5e-4
+EPS = 1e-4
 
 
 def _ada(**kw):
