@@ -312,7 +312,9 @@ def adaptive_measure():
     res = {"tiles": int(len(lv)), "levels_hist": np.bincount(np.log2(lv).astype(int), minlength=5).tolist(),
            "cells_base": int(a.value("cells_base")), "cells_evaluated": int(a.value("cells_evaluated")),
            "audited": int(a.value("audited")), "audit_failures": int(a.value("audit_failures")),
-           "t_base_ms": a.value("t_base") * 1e3, "t_adapt_ms": a.value("t_adapt") * 1e3}
+           "t_base_ms": a.value("t_base") * 1e3, "t_adapt_ms": a.value("t_adapt") * 1e3,
+           "t_select_ms": a.value("t_select") * 1e3, "t_audit_ms": a.value("t_audit") * 1e3,
+           "t_refine_deposit_ms": a.value("t_refine_deposit") * 1e3}
     a.close()
     u16 = irs_b200.AdaptiveIPM(policy="uniform", level=16, audit_fraction=0.0, **cfg)
     u16.run()

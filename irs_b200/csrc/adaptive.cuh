@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(256) ada_refine_corners(AdaGeom g, ShootParams
 // over the map pixels in the window, W_c being the tile's deposit at level 2^c
 // (the reference is below).
 constexpr int kAdaWindow = 256;       // pixels per side of a tile's window
-constexpr int kAdaWindowLarge = 1024; // window of a chunk holding a tile whose image needs more
+constexpr int kAdaWindowLarge = 512;  // window of a chunk holding a tile whose image needs more
 constexpr int kAdaWindowMargin = 2;
 constexpr double kAdaMapWeight = 20.0;  // mode 2: weight of the map-relative error
 

@@ -48,11 +48,14 @@ class AdaptiveIPM {
   std::vector<int> level, predicted;  // per tile, subdivision 1..16
   long long cells_base = 0, cells_evaluated = 0, audit_cells = 0;
   int audited = 0, audit_failures = 0;
-  double t_base = 0, t_adapt = 0;
+  double t_base = 0, t_adapt = 0;                          // seconds
+  double t_select = 0, t_audit = 0, t_refine_deposit = 0;  // parts of t_adapt
 
   ~AdaptiveIPM() {
     if (e0_) cudaEventDestroy(e0_);
     if (e1_) cudaEventDestroy(e1_);
+    if (ea_) cudaEventDestroy(ea_);
+    if (eb_) cudaEventDestroy(eb_);
   }
 
   int num_tiles() const { return ntx * nty; }
@@ -66,19 +69,28 @@ class AdaptiveIPM {
     if (!e0_) {
       IRSB_CKR(cudaEventCreate(&e0_));
       IRSB_CKR(cudaEventCreate(&e1_));
+      IRSB_CKR(cudaEventCreate(&ea_));
+      IRSB_CKR(cudaEventCreate(&eb_));
     }
     setup_geometry();
     base_map_ready_ = false;
     IRSB_CKR(cudaEventRecord(e0_, s));
     if (!features()) return false;
     if (!choose_levels()) return false;
+    IRSB_CKR(cudaEventRecord(ea_, s));
     if (!audit()) return false;
+    IRSB_CKR(cudaEventRecord(eb_, s));
     if (!deposit()) return false;
     IRSB_CKR(cudaEventRecord(e1_, s));
     IRSB_CKR(cudaEventSynchronize(e1_));
-    float ms = 0;
+    float ms = 0, m1 = 0, m2 = 0;
     IRSB_CKR(cudaEventElapsedTime(&ms, e0_, e1_));
+    IRSB_CKR(cudaEventElapsedTime(&m1, e0_, ea_));
+    IRSB_CKR(cudaEventElapsedTime(&m2, ea_, eb_));
     t_adapt = ms * 1e-3;
+    t_select = m1 * 1e-3;
+    t_audit = m2 * 1e-3;
+    t_refine_deposit = (ms - m1 - m2) * 1e-3;
     if (verbose >= 1) {
       long long hist[kAdaLevels] = {0};
       for (int v : level) hist[__builtin_ctz(v)]++;
@@ -124,7 +136,7 @@ class AdaptiveIPM {
   const T* map_device() const { return d_map_.p; }
 
  private:
-  cudaEvent_t e0_ = nullptr, e1_ = nullptr;
+  cudaEvent_t e0_ = nullptr, e1_ = nullptr, ea_ = nullptr, eb_ = nullptr;
   AdaGeom g_{};
   ShootParams sp_{};
   bool generic_ = false;

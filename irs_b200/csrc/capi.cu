@@ -432,6 +432,9 @@ double ada_get_value(void* a, const char* name) {
   if (n == "audit_failures") return ad->audit_failures;
   if (n == "t_base") return ad->t_base;
   if (n == "t_adapt") return ad->t_adapt;
+  if (n == "t_select") return ad->t_select;
+  if (n == "t_audit") return ad->t_audit;
+  if (n == "t_refine_deposit") return ad->t_refine_deposit;
   if (n == "tolerance") return ad->eps;
   return get_value(&ad->base, name);
 }

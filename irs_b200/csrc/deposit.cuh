@@ -82,6 +82,7 @@ struct Tri {
   int ox, oy;
   int rlo, nrows;   // first row (relative) and number of rows to visit
   int map;          // 0 total, 1 minima, 2 saddles
+  int single;       // 1: the triangle lies inside one map pixel, (ox, oy)
 };
 
 template <typename D>
@@ -101,6 +102,7 @@ __device__ __forceinline__ Tri<D> setup_triangle(double ax, double ay, double bx
   t.rlo = 0;
   t.ox = t.oy = 0;
   t.map = 0;
+  t.single = 0;
   t.scale = D(0);
   for (int k = 0; k < 3; k++) t.x[k] = t.y[k] = t.sl[k] = t.idy[k] = D(0);
   if (isnan(ax) || isnan(ay) || isnan(bx) || isnan(by) || isnan(cx) || isnan(cy)) return t;
@@ -154,6 +156,8 @@ __device__ __forceinline__ Tri<D> setup_triangle(double ax, double ay, double bx
   if (rhi > npy - 1 - oy) rhi = npy - 1 - oy;
   t.rlo = rlo;
   t.nrows = rhi >= rlo ? rhi - rlo + 1 : 0;
+  // inside one pixel of the map: all its area goes there
+  t.single = (t.nrows == 1 && mxx < D(1) && mxy < D(1) && ox >= 0 && ox < npx) ? 1 : 0;
   return t;
 }
 
@@ -307,12 +311,14 @@ __device__ __forceinline__ void deposit_row(const Tri<D>& t, int r, int npx, Dep
 
 // Cells of an ncx x ncy lattice whose (ncx+1) x (ncy+1) corner positions are in
 // `verts`. A warp takes 32 consecutive cells and handles their first
-// triangles, then their second triangles: each lane prepares one triangle and
-// deposits its first row; the warp then scans the counts of the remaining
-// rows and works through those (triangle, row) items 32 at a time, each lane
-// finding its item's owner lane by a binary search over the scan and reading
-// the triangle through shuffles, so a triangle with many rows is spread over
-// the warp instead of holding one lane.
+// triangles, then their second triangles: each lane prepares one triangle; a
+// triangle inside one pixel is deposited at once; unless most lanes had such a
+// triangle, each lane deposits its own triangle's first row; the warp then
+// scans the counts of the remaining rows and works through those (triangle,
+// row) items 32 at a time, each lane finding its item's owner lane by a
+// binary search over the scan and reading the triangle through shuffles, so
+// a triangle with many rows is spread over the warp instead of holding one
+// lane.
 // The 32 cells [base, base + 32) of an ncx-wide lattice whose corner rows are
 // vx apart (whole warp; lanes past ncells idle).
 template <typename D>
@@ -342,16 +348,26 @@ __device__ __forceinline__ void deposit_warp_cells(const double2* __restrict__ v
 #pragma unroll 1
   for (int half = 0; half < 2; half++) {
     Tri<D> mine;
-    mine.nrows = 0;
+    mine.nrows = 0;  // idle lanes (past the last cell) deposit nothing
+    mine.single = 0;
     if (c < ncells) {
       mine = half == 0 ? setup_triangle<D>(y0.x, y0.y, y1.x, y1.y, y2.x, y2.y, factor, npx, npy, parities != 0)
                        : setup_triangle<D>(y2.x, y2.y, y3.x, y3.y, y0.x, y0.y, factor, npx, npy, parities != 0);
     }
-    if (mine.nrows > 0) {
+    // a triangle inside one pixel puts factor there (its whole area)
+    if (mine.single) {
+      DepositMaps M = mine.map == 0 ? m_total : (mine.map == 1 ? m_min : m_sad);
+      atomicAdd(M.acc + (long long)mine.oy * npx + mine.ox, RN<D>::to_fix(RN<D>::mul(factor, D(kFixScale))));
+    }
+    // Mostly one-pixel triangles (fine lattices): share out every row of the
+    // others. Otherwise each lane first deposits its own triangle's first row.
+    const bool share_all = __popc(__ballot_sync(0xffffffffu, mine.single != 0)) >= 16;
+    const int first = share_all ? 0 : 1;
+    if (!share_all && mine.nrows > 0 && !mine.single) {
       DepositMaps M = mine.map == 0 ? m_total : (mine.map == 1 ? m_min : m_sad);
       deposit_row<D>(mine, mine.rlo, npx, M);
     }
-    const int extra = mine.nrows > 1 ? mine.nrows - 1 : 0;
+    const int extra = mine.single ? 0 : (mine.nrows > first ? mine.nrows - first : 0);
     int incl = extra;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -386,7 +402,7 @@ __device__ __forceinline__ void deposit_warp_cells(const double2* __restrict__ v
       t.map = __shfl_sync(0xffffffffu, mine.map, owner);
       if (item < total) {
         DepositMaps M = t.map == 0 ? m_total : (t.map == 1 ? m_min : m_sad);
-        deposit_row<D>(t, t.rlo + 1 + (item - before), npx, M);
+        deposit_row<D>(t, t.rlo + first + (item - before), npx, M);
       }
     }
   }
@@ -394,12 +410,14 @@ __device__ __forceinline__ void deposit_warp_cells(const double2* __restrict__ v
 
 // Cells of an ncx x ncy lattice whose (ncx+1) x (ncy+1) corner positions are in
 // `verts`. A warp takes 32 consecutive cells and handles their first
-// triangles, then their second triangles: each lane prepares one triangle and
-// deposits its first row; the warp then scans the counts of the remaining
-// rows and works through those (triangle, row) items 32 at a time, each lane
-// finding its item's owner lane by a binary search over the scan and reading
-// the triangle through shuffles, so a triangle with many rows is spread over
-// the warp instead of holding one lane.
+// triangles, then their second triangles: each lane prepares one triangle; a
+// triangle inside one pixel is deposited at once; unless most lanes had such a
+// triangle, each lane deposits its own triangle's first row; the warp then
+// scans the counts of the remaining rows and works through those (triangle,
+// row) items 32 at a time, each lane finding its item's owner lane by a
+// binary search over the scan and reading the triangle through shuffles, so
+// a triangle with many rows is spread over the warp instead of holding one
+// lane.
 template <typename D>
 __global__ void __launch_bounds__(256, sizeof(D) == 4 ? 4 : 2)
     ipm_deposit_cells(const double2* __restrict__ verts, long long ncx, long long ncy, D factor, int npx, int npy,
