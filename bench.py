@@ -293,8 +293,9 @@ def adaptive_measure():
     network-chosen map against the uniform-fine (level 16) map; the cells a
     uniform subdivision needs for the same error (interpolated between the
     uniform levels' errors); and the plain uniform FP64 form at that cost,
-    its tree and expansions timed once and its shooting per cell timed on a
-    band of lattice rows at level 4 (num_rays_y = 16)."""
+    its tree and expansions timed once and its shooting per cell timed on
+    four bands of lattice rows spread over the lattice at level 4
+    (num_rays_y = 16)."""
     import irs_b200
 
     def rel_err(mu, ref):
@@ -348,14 +349,20 @@ def adaptive_measure():
     p.derive()
     ny = int(p.value("num_ray_threads_2"))
     nx = int(p.value("num_ray_threads_1"))
-    rows = max(1, ny // 16)
-    p.lib.set_band(p.obj, 0, rows)
-    p.run()
-    tb = p.rerun(1)
-    shoot = p.value("t_lattice") + p.value("t_deposit")
+    rows = max(1, ny // 64)
+    shoot, tree = 0.0, None
+    for k in range(4):  # four bands spread over the lattice (its edges map far off the map)
+        lo = (2 * k + 1) * ny // 8 - rows // 2
+        p.lib.set_band(p.obj, lo, lo + rows)
+        if k == 0:
+            p.run()
+        tb = p.rerun(1)
+        sh = p.value("t_lattice") + p.value("t_deposit")
+        shoot += sh
+        tree = tb - sh
     p.close()
-    per_cell = shoot / (float(nx) * rows)
-    t_plain = (tb - shoot) + per_cell * res["cells_base"] * f_match
+    per_cell = shoot / (float(nx) * rows * 4)
+    t_plain = tree + per_cell * res["cells_base"] * f_match
     res.update({"plain_fp64_s_at_matching_cells": t_plain, "plain_fp64_ns_per_cell": per_cell * 1e9,
                 "adaptive_s": t_ada,
                 "effective_cells_per_s_adaptive": res["cells_base"] * f_match / t_ada,

@@ -98,7 +98,8 @@ class AdaptiveIPM:
     are those of IPM (keyword arguments)."""
 
     def __init__(self, network=None, policy="network", level=1, levels=None, tolerance=1e-4,
-                 audit_fraction=0.01, audit_seed=1, refine_capacity=0, quantile=0.8, error_mode=0, max_level=8, is_double=False,
+                 audit_fraction=0.01, audit_seed=1, refine_capacity=0, quantile=0.8, error_mode=0, max_level=8,
+                 tiled_min=64, is_double=False,
                  verbose=0,
                  **ipm_kwargs):
         self.is_double = bool(is_double)
@@ -123,6 +124,7 @@ class AdaptiveIPM:
         if max_level not in LEVELS:
             raise ValueError("max_level must be 1, 2, 4, 8 or 16")
         self.lib.ada_set_max_level(self.h, int(max_level))
+        self.lib.ada_set_tiled_min(self.h, int(tiled_min))
         self.lib.ada_set_audit(self.h, float(audit_fraction), int(audit_seed))
         self.lib.ada_set_refine_capacity(self.h, int(refine_capacity))
 

@@ -216,6 +216,77 @@ __global__ void __launch_bounds__(256) ada_refine_corners(AdaGeom g, ShootParams
   }
 }
 
+// After the tiled pass over the level-s lattice (shoot_f32_tiles): base points
+// of the tiles in `list` take the base lattice's positions (so that every
+// level shares them exactly), and points on an edge shared with a coarser
+// neighbour move onto that neighbour's edge segment, between the tile's own
+// positions at the neighbour's corners (the same lattice points the
+// neighbour holds). One thread per corner; the points written (base points,
+// edge points between coarse corners) and the points read (base points from
+// the base lattice, coarse corners) are disjoint.
+__global__ void __launch_bounds__(256) ada_fixup_corners(AdaGeom g, const double2* __restrict__ base_verts,
+                                                         const int* __restrict__ tile_level,
+                                                         const int* __restrict__ list, int nlist, int s,
+                                                         long long stride, double2* __restrict__ out) {
+  const int side = kAdaTile * s + 1;
+  const long long per_tile = (long long)side * side;
+  const long long total = per_tile * nlist;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int slot = int(q / per_tile);
+    const int rem = int(q - (long long)slot * per_tile);
+    const int b = rem / side, a = rem - b * side;
+    const int t = list[slot];
+    const int tx = t % g.ntx, ty = t / g.ntx;
+    const int ncx_t = int(llmin_(kAdaTile, g.ncx - (long long)tx * kAdaTile));
+    const int ncy_t = int(llmin_(kAdaTile, g.ncy - (long long)ty * kAdaTile));
+    const int wa = ncx_t * s, hb = ncy_t * s;
+    if (a > wa || b > hb) continue;
+    double2* P = out + (long long)slot * stride;
+    const long long W = wa + 1;
+    const long long i0 = (long long)tx * kAdaTile, j0 = (long long)ty * kAdaTile;
+    if (a % s == 0 && b % s == 0) {
+      P[b * W + a] = base_verts[(j0 + b / s) * (g.ncx + 1) + i0 + a / s];
+      continue;
+    }
+    int nlev = s;
+    bool along_b = false;
+    if (a == 0 && tx > 0) {
+      nlev = tile_level[t - 1];
+      along_b = true;
+    } else if (a == wa && tx + 1 < g.ntx && wa == kAdaTile * s) {
+      nlev = tile_level[t + 1];
+      along_b = true;
+    } else if (b == 0 && ty > 0) {
+      nlev = tile_level[t - g.ntx];
+    } else if (b == hb && ty + 1 < g.nty && hb == kAdaTile * s) {
+      nlev = tile_level[t + g.ntx];
+    }
+    if (nlev >= s) continue;
+    const int step = s / nlev;
+    const int u = along_b ? b : a;
+    if (u % step == 0) continue;
+    const int u0 = (u / step) * step, u1 = u0 + step;
+    auto at = [&](int aa, int bb) -> double2 {
+      if (aa % s == 0 && bb % s == 0) return base_verts[(j0 + bb / s) * (g.ncx + 1) + i0 + aa / s];
+      return P[bb * W + aa];
+    };
+    const double2 p0 = along_b ? at(a, u0) : at(u0, b);
+    const double2 p1 = along_b ? at(a, u1) : at(u1, b);
+    const double f = double(u - u0) / double(step);
+    P[b * W + a] = make_double2(p0.x + (p1.x - p0.x) * f, p0.y + (p1.y - p0.y) * f);
+  }
+}
+
+// slot[t] = position of tile t in list (ada_slots_set), -1 for the other
+// tiles (ada_slots_clear).
+__global__ void ada_slots_clear(int ntiles, int* __restrict__ slot) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) slot[t] = -1;
+}
+__global__ void ada_slots_set(const int* __restrict__ list, int nlist, int* __restrict__ slot) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nlist; k += gridDim.x * blockDim.x) slot[list[k]] = k;
+}
+
 // Deposit error of levels 1, 2, 4, 8 against level 16, tile by tile. Each
 // tile is deposited on its own into a private pixel window at every level
 // (level-s corners are every (16/s)-th level-16 corner), and

@@ -40,6 +40,10 @@ class AdaptiveIPM {
   double audit_fraction = 0.01;  // share of tiles audited per run
   unsigned audit_seed = 1;
   long long refine_cap = 0;      // corner positions in the refinement buffer (0: automatic)
+  // chunks of at least this many tiles of one level are refined by the tiled
+  // lens kernel over the level-s lattice (refine_tiled), smaller ones point by
+  // point (ada_refine_corners)
+  int tiled_min = 64;
   std::vector<float> net_w, net_mu, net_sig;  // FP32 master weights, feature standardisation
   float net_quantile = 0.8f;  // a tile takes the smallest level whose cumulative probability reaches this
 
@@ -146,6 +150,8 @@ class AdaptiveIPM {
   DevVec<double2> d_ref_;
   DevVec<DepositPiece<float>> d_pieces_;
   DevVec<int4> d_win_;
+  DevVec<int> d_slot_;
+  LatticeTiles rtiles_;  // lattice tiles of a refinement pass
   DevVec<unsigned long long> d_acc_, d_diff_, d_wacc_, d_wdiff_, d_bacc_, d_bdiff_;
   bool base_map_ready_ = false;
   DevVec<T> d_map_;
@@ -358,6 +364,51 @@ class AdaptiveIPM {
     return true;
   }
 
+
+  // Corner grids of the tiles `tl` (host, row-major tile order) / `d_tl`
+  // (device) at level sl into d_ref_: the leaf-tiled FP32 lens kernel over
+  // the rows of the level-sl corner lattice that these tiles span, each point
+  // stored in the grids holding it, then ada_fixup_corners.
+  bool refine_tiled(int sl, const int* tl, const int* d_tl, int n) {
+    cudaStream_t s = base.stream_;
+    const int nt = num_tiles();
+    const long long per = (long long)(kAdaTile * sl + 1) * (kAdaTile * sl + 1);
+    if (!d_slot_.alloc_exact(nt)) return false;
+    ada_slots_clear<<<std::max(1, std::min(ceil_div(nt, 256), 148 * 8)), 256, 0, s>>>(nt, d_slot_.p);
+    ada_slots_set<<<std::max(1, ceil_div(n, 256)), 256, 0, s>>>(d_tl, n, d_slot_.p);
+    const int ty_a = tl[0] / ntx, ty_b = tl[n - 1] / ntx;
+    const long long nxs = g_.ncx * sl + 1, nys = g_.ncy * sl + 1;
+    const long long jlo = (long long)ty_a * kAdaTile * sl;
+    const long long jhi = std::min<long long>(((long long)ty_b + 1) * kAdaTile * sl + 1, nys);
+    ShootParams sps = sp_;
+    sps.rhs_x = sp_.rhs_x / sl;  // exact: sl is a power of two
+    sps.rhs_y = sp_.rhs_y / sl;
+    sps.nx = nxs;
+    sps.ny = nys;
+    sps.jbase = 0;
+    if (!build_lattice_tiles<T>(rtiles_, base.leaves_, base.tree_, sps.base_x, sps.base_y, sps.rhs_x, sps.rhs_y, nxs,
+                                nys, jlo, jhi, s))
+      return false;
+    LeafPtrs lp = base.leaf_ptrs();
+    lp.rect = rtiles_.rect.p;
+    lp.tile_off = rtiles_.tile_off.p;
+    lp.table = rtiles_.table.p;
+    const TileStore st{d_slot_.p, sl, ntx, nty, g_.ncx, g_.ncy, per, d_ref_.p};
+    if (rtiles_.total > 0) {
+      const int grid = int(std::max<long long>(1, std::min<long long>(rtiles_.total, 148LL * 8)));
+      if (generic_)
+        shoot_f32_tiles<true><<<grid, kShootThreads, 0, s>>>(sps, lp, rtiles_.total, st);
+      else
+        shoot_f32_tiles<false><<<grid, kShootThreads, 0, s>>>(sps, lp, rtiles_.total, st);
+      IRSB_LAUNCH_CK("shoot_f32_tiles");
+    }
+    const long long total = per * n;
+    const int grid = int(std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 32)));
+    ada_fixup_corners<<<grid, 256, 0, s>>>(g_, base.d_verts_.p, d_level_.p, d_tl, n, sl, per, d_ref_.p);
+    IRSB_LAUNCH_CK("ada_fixup_corners");
+    return true;
+  }
+
   bool deposit() {
     cudaStream_t s = base.stream_;
     const Params<T>& p = base.prm;
@@ -430,7 +481,10 @@ class AdaptiveIPM {
     const DepositMaps M{d_acc_.p, d_diff_.p};
     for (const Launch& L : launches) {
       const double2* verts = base.d_verts_.p;
-      if (L.s > 1) {
+      if (L.s > 1 && L.nlist >= tiled_min) {
+        if (!refine_tiled(L.s, lists.data() + L.list_off, d_list_.p + L.list_off, L.nlist)) return false;
+        verts = d_ref_.p;
+      } else if (L.s > 1) {
         const long long per = (long long)(kAdaTile * L.s + 1) * (kAdaTile * L.s + 1);
         const long long total = per * L.nlist;
         const int grid = int(std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 32)));

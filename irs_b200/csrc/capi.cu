@@ -396,6 +396,7 @@ void ada_set_audit(void* a, double fraction, unsigned seed) {
   static_cast<Ada*>(a)->audit_seed = seed;
 }
 void ada_set_refine_capacity(void* a, long long n) { static_cast<Ada*>(a)->refine_cap = n; }
+void ada_set_tiled_min(void* a, int n) { static_cast<Ada*>(a)->tiled_min = n; }
 void ada_set_network(void* a, const float* w, const float* mu, const float* sig) {
   Ada* ad = static_cast<Ada*>(a);
   ad->net_w.assign(w, w + irsb::kMlpParams);

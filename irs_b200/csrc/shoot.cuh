@@ -72,14 +72,49 @@ struct TileInfo {
   int leaf, i0, j0, ni, nj;
 };
 
-// Destination of a tile's results: IRS maps, or the IPM corner buffer whose
-// row 0 is lattice row vrow0.
+// Corner buffers of refined tiles (adaptive IPM): a point (i, j) of the
+// level-s corner lattice belongs to every tile of level s whose corner grid
+// holds it (up to 4 on tile edges) and is stored in each of their buffers:
+// tile t at out + slot[t] * per, row stride ncell_x(t) * s + 1.
+struct TileStore {
+  const int* slot;  // per tile: buffer slot, -1 when not refined in this pass
+  int s;            // subdivision level
+  int ntx, nty;     // tiles
+  long long ncx, ncy;  // base cells
+  long long per;    // corners per slot
+  double2* out;
+};
+
+__device__ __forceinline__ void tile_store(const TileStore& st, long long i, long long j, double2 v) {
+  const long long side = 32LL * st.s;  // lattice points per tile side
+  const int txh = int(i / side), tyh = int(j / side);
+#pragma unroll
+  for (int dy = 0; dy < 2; dy++) {
+    const int ty = tyh - dy;
+    if (ty < 0 || ty >= st.nty || (dy == 1 && j % side != 0)) continue;
+#pragma unroll
+    for (int dx = 0; dx < 2; dx++) {
+      const int tx = txh - dx;
+      if (tx < 0 || tx >= st.ntx || (dx == 1 && i % side != 0)) continue;
+      const int t = ty * st.ntx + tx;
+      const int k = st.slot[t];
+      if (k < 0) continue;
+      const long long cx = (st.ncx - 32LL * tx) < 32 ? (st.ncx - 32LL * tx) : 32;
+      const long long a = i - tx * side, b = j - ty * side;
+      st.out[k * st.per + b * (cx * st.s + 1) + a] = v;
+    }
+  }
+}
+
+// Destination of a tile's results: IRS maps, the IPM corner buffer whose
+// row 0 is lattice row vrow0, or refined tile buffers (tiles != nullptr).
 struct ShootOut {
   int* pix;
   int* pmin;
   int* psad;
   double2* verts;
   long long vrow0;
+  const TileStore* tiles = nullptr;
 };
 
 __device__ __forceinline__ TileInfo tile_info(const LeafPtrs& lp, long long t) {
@@ -335,7 +370,10 @@ __device__ __forceinline__ void shoot_f32_tile(const ShootParams& sp, const Leaf
           py += (-a_sm.im - sp.kstar * z.im) * scy;
         }
         if (VERT) {
-          o.verts[(size_t)(j - o.vrow0) * (sp.nx) + i] = make_double2(px, double(sp.npy) - py);
+          if (o.tiles)
+            tile_store(*o.tiles, i, j, make_double2(px, double(sp.npy) - py));
+          else
+            o.verts[(size_t)(j - o.vrow0) * (sp.nx) + i] = make_double2(px, double(sp.npy) - py);
         } else {
           if (!(px >= 0.0 && px <= double(sp.npx) && py >= 0.0 && py <= double(sp.npy))) continue;
           bool pmin_ = false;
@@ -374,6 +412,28 @@ __global__ void __launch_bounds__(THREADS) shoot_f32(ShootParams sp, LeafPtrs lp
   const ShootOut o{pix, pmin, psad, verts, sp.jbase};
   for (long long t = blockIdx.x; t < total_tiles; t += gridDim.x)
     shoot_f32_tile<VERT, PAR, GENERIC_SMOOTH, THREADS>(sp, lp, tile_info(lp, t), o, s_near, s_coef);
+}
+
+// The level-s corner lattice restricted to refined tiles: work items whose
+// 32 x 32 block touches no tile with a buffer slot are skipped.
+template <bool GENERIC_SMOOTH>
+__global__ void __launch_bounds__(kShootThreads) shoot_f32_tiles(ShootParams sp, LeafPtrs lp, long long total_tiles,
+                                                                 TileStore st) {
+  __shared__ float4 s_near[kMaxStarsDirect];
+  __shared__ float2 s_coef[kMaxOrder];
+  const ShootOut o{nullptr, nullptr, nullptr, nullptr, 0, &st};
+  const long long side = 32LL * st.s;
+  for (long long t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+    const TileInfo ti = tile_info(lp, t);
+    const int tx0 = int(ti.i0 / side), tx1 = int((ti.i0 + ti.ni - 1) / side);
+    const int ty0 = int(ti.j0 / side), ty1 = int((ti.j0 + ti.nj - 1) / side);
+    bool need = false;  // uniform over the block
+    for (int ty = ty0 > 0 ? ty0 - 1 : 0; ty <= ty1 && ty < st.nty && !need; ty++)
+      for (int tx = tx0 > 0 ? tx0 - 1 : 0; tx <= tx1 && tx < st.ntx && !need; tx++)
+        need = st.slot[ty * st.ntx + tx] >= 0;
+    if (!need) continue;
+    shoot_f32_tile<true, false, GENERIC_SMOOTH>(sp, lp, ti, o, s_near, s_coef);
+  }
 }
 
 // Many realizations in one launch: the tiles of all their leaves form one work

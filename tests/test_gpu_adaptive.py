@@ -39,6 +39,19 @@ def test_level1_equals_plain_map(gpu):
     assert a.value("cells_evaluated") == a.value("cells_base")
 
 
+def test_tiled_and_pointwise_refinement_agree(gpu):
+    # the tiled lens kernel over the level-s lattice and the point-by-point
+    # evaluation compute each refined corner with the same arithmetic
+    rng = np.random.default_rng(5)
+    n = len(_ada(policy="uniform", level=1, audit_fraction=0.0).levels())
+    lv = rng.choice([1, 2, 4, 8], n).astype(np.int32)
+    a = _ada(policy="given", levels=lv, audit_fraction=0.0, tiled_min=1)
+    b = _ada(policy="given", levels=lv, audit_fraction=0.0, tiled_min=1 << 30)
+    mu_a, mu_b = a.magnifications.astype(np.float64), b.magnifications.astype(np.float64)
+    assert np.abs(mu_a - mu_b).max() <= 1e-6 * mu_b.max()
+    assert a.value("cells_evaluated") == b.value("cells_evaluated")
+
+
 def test_uniform_refinement_converges(gpu):
     ref = _ada(policy="uniform", level=16, audit_fraction=0.0).magnifications.astype(np.float64)
     errs = []
