@@ -99,7 +99,7 @@ class AdaptiveIPM:
 
     def __init__(self, network=None, policy="network", level=1, levels=None, tolerance=1e-4,
                  audit_fraction=0.01, audit_seed=1, refine_capacity=0, quantile=0.8, error_mode=0, max_level=8,
-                 tiled_min=64, is_double=False,
+                 tiled_min=1 << 30, is_double=False,
                  verbose=0,
                  **ipm_kwargs):
         self.is_double = bool(is_double)

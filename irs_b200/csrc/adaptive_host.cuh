@@ -43,7 +43,7 @@ class AdaptiveIPM {
   // chunks of at least this many tiles of one level are refined by the tiled
   // lens kernel over the level-s lattice (refine_tiled), smaller ones point by
   // point (ada_refine_corners)
-  int tiled_min = 64;
+  int tiled_min = 1 << 30;
   std::vector<float> net_w, net_mu, net_sig;  // FP32 master weights, feature standardisation
   float net_quantile = 0.8f;  // a tile takes the smallest level whose cumulative probability reaches this
 

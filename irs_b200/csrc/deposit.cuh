@@ -91,12 +91,13 @@ __device__ __forceinline__ D rcp_or_zero(D v) {
 }
 
 // Triangle (a, b, c) in absolute pixel coordinates (row axis flipped) ->
-// Tri, or nrows = 0 when it deposits nothing. Tests of the reference
+// Tri without its reciprocals and scale (setup_tail), or nrows = 0 when it
+// deposits nothing; scale holds the triangle's area. Tests of the reference
 // (ipm_functions.cuh:170-193, polygon.cuh:351-372): NaN corner, |A| >= 1e4
 // * factor, entirely outside the map, zero area.
 template <typename D>
-__device__ __forceinline__ Tri<D> setup_triangle(double ax, double ay, double bx, double by, double cx, double cy,
-                                                 D factor, int npx, int npy, bool parities) {
+__device__ __forceinline__ Tri<D> setup_head(double ax, double ay, double bx, double by, double cx, double cy,
+                                             D factor, int npx, int npy, bool parities) {
   Tri<D> t;
   t.nrows = 0;
   t.rlo = 0;
@@ -141,14 +142,7 @@ __device__ __forceinline__ Tri<D> setup_triangle(double ax, double ay, double bx
   t.y[1] = y1;
   t.x[2] = x2;
   t.y[2] = y2;
-  for (int k = 0; k < 3; k++) {
-    int j = k == 2 ? 0 : k + 1;
-    const D dx = RN<D>::sub(t.x[j], t.x[k]), dy = RN<D>::sub(t.y[j], t.y[k]);
-    t.idy[k] = rcp_or_zero(dy);
-    const D g = RN<D>::mul(dy, rcp_or_zero(dx));
-    t.sl[k] = dabs(g) <= std::numeric_limits<D>::max() ? g : D(0);
-  }
-  t.scale = RN<D>::div(RN<D>::mul(factor, D(kFixScale)), whole);
+  t.scale = whole;  // setup_tail turns it into the fixed-point scale
   t.ox = ox;
   t.oy = oy;
   int rlo = 0 > -oy ? 0 : -oy;
@@ -160,6 +154,57 @@ __device__ __forceinline__ Tri<D> setup_triangle(double ax, double ay, double bx
   t.single = (t.nrows == 1 && mxx < D(1) && mxy < D(1) && ox >= 0 && ox < npx) ? 1 : 0;
   return t;
 }
+
+// Edge reciprocals, slopes and the fixed-point scale of a triangle that
+// deposits row by row (nrows > 0, not single).
+template <typename D>
+__device__ __forceinline__ void setup_tail(Tri<D>& t, D factor) {
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const int j = k == 2 ? 0 : k + 1;
+    const D dx = RN<D>::sub(t.x[j], t.x[k]), dy = RN<D>::sub(t.y[j], t.y[k]);
+    t.idy[k] = rcp_or_zero(dy);
+    const D g = RN<D>::mul(dy, rcp_or_zero(dx));
+    t.sl[k] = dabs(g) <= std::numeric_limits<D>::max() ? g : D(0);
+  }
+  t.scale = RN<D>::div(RN<D>::mul(factor, D(kFixScale)), t.scale);
+}
+
+// Shared-memory staging of the 64 triangles of a warp's 32 cells that go row
+// by row (one array per field: lane k touches word k, no bank conflicts).
+template <typename D>
+struct TriSlots {
+  D x[3][64], y[3][64], area[64];
+  int ox[64], oy[64], rlo[64], nrows[64], map[64];
+  __device__ __forceinline__ void put(int k, const Tri<D>& t) {
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      x[q][k] = t.x[q];
+      y[q][k] = t.y[q];
+    }
+    area[k] = t.scale;
+    ox[k] = t.ox;
+    oy[k] = t.oy;
+    rlo[k] = t.rlo;
+    nrows[k] = t.nrows;
+    map[k] = t.map;
+  }
+  __device__ __forceinline__ void get(int k, Tri<D>& t) const {
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      t.x[q] = x[q][k];
+      t.y[q] = y[q][k];
+    }
+    t.scale = area[k];
+    t.ox = ox[k];
+    t.oy = oy[k];
+    t.rlo = rlo[k];
+    t.nrows = nrows[k];
+    t.map = map[k];
+    t.single = 0;
+  }
+};
+constexpr int kDepositWarps = 8;  // warps per CTA of the deposition kernels (256 threads)
 
 // Geometry of one row strip [rb, rt = rb + 1] of a triangle.
 //   Strip segments: each edge clipped to the strip, endpoints (xa, ya) ->
@@ -309,24 +354,69 @@ __device__ __forceinline__ void deposit_row(const Tri<D>& t, int r, int npx, Dep
   }
 }
 
-// Cells of an ncx x ncy lattice whose (ncx+1) x (ncy+1) corner positions are in
-// `verts`. A warp takes 32 consecutive cells and handles their first
-// triangles, then their second triangles: each lane prepares one triangle; a
-// triangle inside one pixel is deposited at once; unless most lanes had such a
-// triangle, each lane deposits its own triangle's first row; the warp then
-// scans the counts of the remaining rows and works through those (triangle,
-// row) items 32 at a time, each lane finding its item's owner lane by a
-// binary search over the scan and reading the triangle through shuffles, so
-// a triangle with many rows is spread over the warp instead of holding one
-// lane.
+// The rows of the triangles of a warp, one triangle per lane (nrows = 0: none):
+// each lane deposits its own triangle's first row; the warp then scans the
+// counts of the remaining rows and works through those (triangle, row) items
+// 32 at a time, each lane finding its item's owner lane by a binary search
+// over the scan and reading the triangle through shuffles, so a triangle with
+// many rows is spread over the warp instead of holding one lane.
+template <typename D>
+__device__ __forceinline__ void deposit_rows_warp(const Tri<D>& mine, int npx, const DepositMaps& m_total,
+                                                  const DepositMaps& m_min, const DepositMaps& m_sad) {
+  const int lane = threadIdx.x & 31;
+  if (mine.nrows > 0) {
+    const DepositMaps& M = mine.map == 0 ? m_total : (mine.map == 1 ? m_min : m_sad);
+    deposit_row<D>(mine, mine.rlo, npx, M);
+  }
+  const int extra = mine.nrows > 1 ? mine.nrows - 1 : 0;
+  int incl = extra;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  for (int it0 = 0; it0 < total; it0 += 32) {
+    const int item = it0 + lane;
+    int lo = 0, hi = 31;  // owner: first lane whose inclusive count exceeds item
+#pragma unroll
+    for (int step = 0; step < 5; step++) {
+      int mid = (lo + hi) >> 1;
+      int v = __shfl_sync(0xffffffffu, incl, mid);
+      if (v > item) hi = mid;
+      else lo = mid + 1;
+    }
+    const int owner = lo;
+    const int before = __shfl_sync(0xffffffffu, incl - extra, owner);
+    Tri<D> t;
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      t.x[q] = __shfl_sync(0xffffffffu, mine.x[q], owner);
+      t.y[q] = __shfl_sync(0xffffffffu, mine.y[q], owner);
+      t.sl[q] = __shfl_sync(0xffffffffu, mine.sl[q], owner);
+      t.idy[q] = __shfl_sync(0xffffffffu, mine.idy[q], owner);
+    }
+    t.scale = __shfl_sync(0xffffffffu, mine.scale, owner);
+    t.ox = __shfl_sync(0xffffffffu, mine.ox, owner);
+    t.oy = __shfl_sync(0xffffffffu, mine.oy, owner);
+    t.rlo = __shfl_sync(0xffffffffu, mine.rlo, owner);
+    t.map = __shfl_sync(0xffffffffu, mine.map, owner);
+    if (item < total) {
+      const DepositMaps& M = t.map == 0 ? m_total : (t.map == 1 ? m_min : m_sad);
+      deposit_row<D>(t, t.rlo + 1 + (item - before), npx, M);
+    }
+  }
+}
+
 // The 32 cells [base, base + 32) of an ncx-wide lattice whose corner rows are
 // vx apart (whole warp; lanes past ncells idle).
 template <typename D>
 __device__ __forceinline__ void deposit_warp_cells(const double2* __restrict__ verts, long long ncx, long long vx,
                                                    long long ncells, long long base, D factor, int npx, int npy,
                                                    const DepositMaps& m_total, const DepositMaps& m_min,
-                                                   const DepositMaps& m_sad, int parities, long long vstep = 1,
-                                                   double ox = 0.0, double oy = 0.0, double inv_scale = 1.0) {
+                                                   const DepositMaps& m_sad, int parities, TriSlots<D>& stage,
+                                                   long long vstep = 1, double ox = 0.0, double oy = 0.0,
+                                                   double inv_scale = 1.0) {
   const int lane = threadIdx.x & 31;
   const long long c = base + lane;
   double2 y0 = make_double2(0, 0), y1 = y0, y2 = y0, y3 = y0;
@@ -345,88 +435,61 @@ __device__ __forceinline__ void deposit_warp_cells(const double2* __restrict__ v
       y0.y *= inv_scale, y1.y *= inv_scale, y2.y *= inv_scale, y3.y *= inv_scale;
     }
   }
+  // each half's head: a triangle inside one pixel deposits at once, the
+  // others are staged in the warp's slots, compacted in lane order
+  const unsigned lt = (1u << lane) - 1u;
+  int n = 0;
 #pragma unroll 1
   for (int half = 0; half < 2; half++) {
-    Tri<D> mine;
-    mine.nrows = 0;  // idle lanes (past the last cell) deposit nothing
-    mine.single = 0;
+    Tri<D> h;
+    h.nrows = 0;  // idle lanes (past the last cell) deposit nothing
+    h.single = 0;
     if (c < ncells) {
-      mine = half == 0 ? setup_triangle<D>(y0.x, y0.y, y1.x, y1.y, y2.x, y2.y, factor, npx, npy, parities != 0)
-                       : setup_triangle<D>(y2.x, y2.y, y3.x, y3.y, y0.x, y0.y, factor, npx, npy, parities != 0);
+      h = half == 0 ? setup_head<D>(y0.x, y0.y, y1.x, y1.y, y2.x, y2.y, factor, npx, npy, parities != 0)
+                    : setup_head<D>(y2.x, y2.y, y3.x, y3.y, y0.x, y0.y, factor, npx, npy, parities != 0);
     }
-    // a triangle inside one pixel puts factor there (its whole area)
-    if (mine.single) {
-      DepositMaps M = mine.map == 0 ? m_total : (mine.map == 1 ? m_min : m_sad);
-      atomicAdd(M.acc + (long long)mine.oy * npx + mine.ox, RN<D>::to_fix(RN<D>::mul(factor, D(kFixScale))));
+    if (h.single) {
+      const DepositMaps& M = h.map == 0 ? m_total : (h.map == 1 ? m_min : m_sad);
+      atomicAdd(M.acc + (long long)h.oy * npx + h.ox, RN<D>::to_fix(RN<D>::mul(factor, D(kFixScale))));
     }
-    // Mostly one-pixel triangles (fine lattices): share out every row of the
-    // others. Otherwise each lane first deposits its own triangle's first row.
-    const bool share_all = __popc(__ballot_sync(0xffffffffu, mine.single != 0)) >= 16;
-    const int first = share_all ? 0 : 1;
-    if (!share_all && mine.nrows > 0 && !mine.single) {
-      DepositMaps M = mine.map == 0 ? m_total : (mine.map == 1 ? m_min : m_sad);
-      deposit_row<D>(mine, mine.rlo, npx, M);
-    }
-    const int extra = mine.single ? 0 : (mine.nrows > first ? mine.nrows - first : 0);
-    int incl = extra;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int v = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += v;
-    }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    for (int it0 = 0; it0 < total; it0 += 32) {
-      const int item = it0 + lane;
-      int lo = 0, hi = 31;  // owner: first lane whose inclusive count exceeds item
-#pragma unroll
-      for (int step = 0; step < 5; step++) {
-        int mid = (lo + hi) >> 1;
-        int v = __shfl_sync(0xffffffffu, incl, mid);
-        if (v > item) hi = mid;
-        else lo = mid + 1;
-      }
-      const int owner = lo;
-      const int before = __shfl_sync(0xffffffffu, incl - extra, owner);
-      Tri<D> t;
-#pragma unroll
-      for (int q = 0; q < 3; q++) {
-        t.x[q] = __shfl_sync(0xffffffffu, mine.x[q], owner);
-        t.y[q] = __shfl_sync(0xffffffffu, mine.y[q], owner);
-        t.sl[q] = __shfl_sync(0xffffffffu, mine.sl[q], owner);
-        t.idy[q] = __shfl_sync(0xffffffffu, mine.idy[q], owner);
-      }
-      t.scale = __shfl_sync(0xffffffffu, mine.scale, owner);
-      t.ox = __shfl_sync(0xffffffffu, mine.ox, owner);
-      t.oy = __shfl_sync(0xffffffffu, mine.oy, owner);
-      t.rlo = __shfl_sync(0xffffffffu, mine.rlo, owner);
-      t.map = __shfl_sync(0xffffffffu, mine.map, owner);
-      if (item < total) {
-        DepositMaps M = t.map == 0 ? m_total : (t.map == 1 ? m_min : m_sad);
-        deposit_row<D>(t, t.rlo + first + (item - before), npx, M);
-      }
-    }
+    const bool cx = h.nrows > 0 && !h.single;
+    const unsigned b = __ballot_sync(0xffffffffu, cx);
+    if (cx) stage.put(n + __popc(b & lt), h);
+    n += __popc(b);
   }
+  __syncwarp();
+  // the staged ones go row by row, one per lane: one round when at most 32
+  // of the warp's 64 triangles need it (fine lattices), else two
+  for (int r0 = 0; r0 < n; r0 += 32) {
+    Tri<D> mine;
+    mine.nrows = 0;
+    if (r0 + lane < n) {
+      stage.get(r0 + lane, mine);
+      setup_tail(mine, factor);
+    }
+    deposit_rows_warp<D>(mine, npx, m_total, m_min, m_sad);
+  }
+  __syncwarp();  // slots free for the warp's next cells
 }
 
 // Cells of an ncx x ncy lattice whose (ncx+1) x (ncy+1) corner positions are in
-// `verts`. A warp takes 32 consecutive cells and handles their first
-// triangles, then their second triangles: each lane prepares one triangle; a
-// triangle inside one pixel is deposited at once; unless most lanes had such a
-// triangle, each lane deposits its own triangle's first row; the warp then
-// scans the counts of the remaining rows and works through those (triangle,
-// row) items 32 at a time, each lane finding its item's owner lane by a
-// binary search over the scan and reading the triangle through shuffles, so
-// a triangle with many rows is spread over the warp instead of holding one
-// lane.
+// `verts`. A warp takes 32 consecutive cells; each lane classifies the two
+// triangles of its cell (setup_head); a triangle inside one pixel is
+// deposited at once; the others are staged in shared memory, compacted, and
+// then get their reciprocals and scale (setup_tail) and go row by row
+// (deposit_rows_warp), one per lane: one round when at most 32 of the warp's
+// 64 triangles need it (fine lattices), else two.
 template <typename D>
-__global__ void __launch_bounds__(256, sizeof(D) == 4 ? 4 : 2)
+__global__ void __launch_bounds__(kDepositWarps * 32, sizeof(D) == 4 ? 4 : 2)
     ipm_deposit_cells(const double2* __restrict__ verts, long long ncx, long long ncy, D factor, int npx, int npy,
                       DepositMaps m_total, DepositMaps m_min, DepositMaps m_sad, int parities) {
   const long long ncells = ncx * ncy;
   const long long warp0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  __shared__ TriSlots<D> slots[kDepositWarps];
+  TriSlots<D>& stage = slots[threadIdx.x >> 5];
   for (long long base = warp0 * 32; base < ncells; base += nwarps * 32)
-    deposit_warp_cells<D>(verts, ncx, ncx + 1, ncells, base, factor, npx, npy, m_total, m_min, m_sad, parities);
+    deposit_warp_cells<D>(verts, ncx, ncx + 1, ncells, base, factor, npx, npy, m_total, m_min, m_sad, parities, stage);
 }
 
 // A block of cells inside a pass of the batched (or adaptive) deposition: its
@@ -448,12 +511,14 @@ struct DepositPiece {
 // of the pass; a chunk's piece is found by a binary search over chunk0.
 // Realization r accumulates into the maps at r * map_stride / r * diff_stride.
 template <typename D>
-__global__ void __launch_bounds__(256, sizeof(D) == 4 ? 4 : 2)
+__global__ void __launch_bounds__(kDepositWarps * 32, sizeof(D) == 4 ? 4 : 2)
     ipm_deposit_batch(const double2* __restrict__ verts, const DepositPiece<D>* __restrict__ pieces, int npieces,
                       long long nchunks, int npx, int npy, DepositMaps maps, long long map_stride,
                       long long diff_stride) {
   const long long warp0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  __shared__ TriSlots<D> slots[kDepositWarps];
+  TriSlots<D>& stage = slots[threadIdx.x >> 5];
   for (long long g = warp0; g < nchunks; g += nwarps) {
     int lo = 0, hi = npieces - 1;  // last piece with chunk0 <= g
     while (lo < hi) {
@@ -464,7 +529,7 @@ __global__ void __launch_bounds__(256, sizeof(D) == 4 ? 4 : 2)
     const DepositPiece<D> pc = pieces[lo];
     const DepositMaps M{maps.acc + pc.r * map_stride, maps.diff + pc.r * diff_stride};
     deposit_warp_cells<D>(verts + pc.voff, pc.ncx, pc.vstride, pc.ncx * pc.ncy, (g - pc.chunk0) * 32, pc.factor,
-                          npx, npy, M, M, M, 0, pc.vstep, pc.ox, pc.oy, pc.inv_scale);
+                          npx, npy, M, M, M, 0, stage, pc.vstep, pc.ox, pc.oy, pc.inv_scale);
   }
 }
 

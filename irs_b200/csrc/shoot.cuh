@@ -86,21 +86,23 @@ struct TileStore {
 };
 
 __device__ __forceinline__ void tile_store(const TileStore& st, long long i, long long j, double2 v) {
-  const long long side = 32LL * st.s;  // lattice points per tile side
-  const int txh = int(i / side), tyh = int(j / side);
+  // lattice indices fit 32 bits (below 32 * 16 * 2^16); side is a power of two
+  const int side = 32 * st.s, sh = __ffs(side) - 1;  // lattice points per tile side
+  const int ii = int(i), jj = int(j);
+  const int txh = ii >> sh, tyh = jj >> sh;
+  const bool on_x = (ii & (side - 1)) == 0, on_y = (jj & (side - 1)) == 0;
 #pragma unroll
   for (int dy = 0; dy < 2; dy++) {
     const int ty = tyh - dy;
-    if (ty < 0 || ty >= st.nty || (dy == 1 && j % side != 0)) continue;
+    if (ty < 0 || ty >= st.nty || (dy == 1 && !on_y)) continue;
 #pragma unroll
     for (int dx = 0; dx < 2; dx++) {
       const int tx = txh - dx;
-      if (tx < 0 || tx >= st.ntx || (dx == 1 && i % side != 0)) continue;
-      const int t = ty * st.ntx + tx;
-      const int k = st.slot[t];
+      if (tx < 0 || tx >= st.ntx || (dx == 1 && !on_x)) continue;
+      const int k = st.slot[ty * st.ntx + tx];
       if (k < 0) continue;
       const long long cx = (st.ncx - 32LL * tx) < 32 ? (st.ncx - 32LL * tx) : 32;
-      const long long a = i - tx * side, b = j - ty * side;
+      const long long a = ii - tx * side, b = jj - ty * side;
       st.out[k * st.per + b * (cx * st.s + 1) + a] = v;
     }
   }
