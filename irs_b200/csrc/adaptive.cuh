@@ -50,6 +50,7 @@ struct DescentPtrs {
   const T* cy;
   const int* child0;
   const long long* leaf_of_node;  // exclusive scan of the leaf flags
+  const int* tile_leaf;           // per tile: the leaf owning all its points, or -1 (nullptr: not known)
 };
 
 template <typename T>
@@ -153,7 +154,8 @@ __device__ __forceinline__ double2 tile_corner(const AdaGeom& g, const ShootPara
   const long long F = (i0 * kAdaMaxLevel) + (long long)a * (kAdaMaxLevel / s);
   const long long G = (j0 * kAdaMaxLevel) + (long long)b * (kAdaMaxLevel / s);
   const double x = fine_coord(g.base_x, g.rhs_x, F), y = fine_coord(g.base_y, g.rhs_y, G);
-  return eval_point_f32<GENERIC_SMOOTH>(sp, lp, descend_leaf(dp, x, y), x, y);
+  const int own = dp.tile_leaf ? dp.tile_leaf[ty * g.ntx + tx] : -1;  // the descent's answer, when uniform
+  return eval_point_f32<GENERIC_SMOOTH>(sp, lp, own >= 0 ? own : descend_leaf(dp, x, y), x, y);
 }
 
 // Refined corner grids of the tiles in `list` (all at level s), written at
@@ -448,7 +450,8 @@ __global__ void __launch_bounds__(256) ada_window_errors(AdaGeom g, const int* _
 //      the tile's 4 corners to the map), 0 when they overlap the map
 template <typename T>
 __global__ void ada_features(AdaGeom g, ShootParams sp, LeafPtrs lp, DescentPtrs<T> dp,
-                             const double2* __restrict__ base_verts, float* __restrict__ feat) {
+                             const double2* __restrict__ base_verts, float* __restrict__ feat,
+                             int* __restrict__ tile_leaf) {
   const int ntiles = g.ntx * g.nty;
   const double cellpx = 2.0 * sp.rhs_x * sp.npx / (2.0 * sp.hly_re);  // unlensed cell width in pixels
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
@@ -478,6 +481,19 @@ __global__ void ada_features(AdaGeom g, ShootParams sp, LeafPtrs lp, DescentPtrs
     const double xc = g.base_x + 2.0 * (g.rhs_x * (double(i0) + 0.5 * double(ilast - i0 + 1)));
     const double yc = g.base_y + 2.0 * (g.rhs_y * (double(j0) + 0.5 * double(jlast - j0 + 1)));
     const int leaf = descend_leaf(dp, xc, yc);
+    {
+      // The points of the tile at any level lie in the box spanned by its
+      // extreme fine coordinates (fine_coord is monotone in the index). A
+      // leaf's points form a box of the descent's comparisons, so when both
+      // extreme corners descend to one leaf every point of the tile does.
+      const double xa = fine_coord(g.base_x, g.rhs_x, i0 * kAdaMaxLevel);
+      const double xb = fine_coord(g.base_x, g.rhs_x, (ilast + 1) * kAdaMaxLevel);
+      const double ya = fine_coord(g.base_y, g.rhs_y, j0 * kAdaMaxLevel);
+      const double yb = fine_coord(g.base_y, g.rhs_y, (jlast + 1) * kAdaMaxLevel);
+      const int la = descend_leaf(dp, fmin(xa, xb), fmin(ya, yb));
+      const int lb = descend_leaf(dp, fmax(xa, xb), fmax(ya, yb));
+      tile_leaf[t] = la == lb ? la : -1;
+    }
     const int nn = lp.nnear[leaf];
     double dn = 1e300;
     const double lcx = lp.cx[leaf], lcy = lp.cy[leaf];

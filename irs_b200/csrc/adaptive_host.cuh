@@ -155,6 +155,8 @@ class AdaptiveIPM {
   DevVec<unsigned long long> d_acc_, d_diff_, d_wacc_, d_wdiff_, d_bacc_, d_bdiff_;
   bool base_map_ready_ = false;
   DevVec<T> d_map_;
+  DevVec<int> d_tile_leaf_;  // per tile: the leaf owning all its points, or -1
+  bool tile_leaf_ready_ = false;
 
   void setup_geometry() {
     const Params<T>& p = base.prm;
@@ -169,7 +171,8 @@ class AdaptiveIPM {
   }
 
   DescentPtrs<T> descent() const {
-    return DescentPtrs<T>{base.tree_.cx.p, base.tree_.cy.p, base.tree_.child0.p, base.leaves_.pos.p};
+    return DescentPtrs<T>{base.tree_.cx.p, base.tree_.cy.p, base.tree_.child0.p, base.leaves_.pos.p,
+                          tile_leaf_ready_ ? d_tile_leaf_.p : nullptr};
   }
 
   int tile_cells_x(int t) const { return int(std::min<long long>(kAdaTile, g_.ncx - (long long)(t % ntx) * kAdaTile)); }
@@ -184,11 +187,13 @@ class AdaptiveIPM {
 
   bool features() {
     const int nt = num_tiles();
-    if (!d_feat_.alloc_exact((size_t)nt * kAdaFeatures)) return false;
+    if (!d_feat_.alloc_exact((size_t)nt * kAdaFeatures) || !d_tile_leaf_.alloc_exact(nt)) return false;
     const int grid = std::max(1, std::min(ceil_div(nt, 128), 148 * 8));
+    tile_leaf_ready_ = false;
     ada_features<T><<<grid, 128, 0, base.stream_>>>(g_, sp_, base.leaf_ptrs(), descent(), base.d_verts_.p,
-                                                    d_feat_.p);
+                                                    d_feat_.p, d_tile_leaf_.p);
     IRSB_LAUNCH_CK("ada_features");
+    tile_leaf_ready_ = true;
     return true;
   }
 

@@ -116,7 +116,7 @@ __device__ __forceinline__ Tri<D> setup_head(double ax, double ay, double bx, do
   s = RN<D>::add(s, RN<D>::sub(RN<D>::mul(RN<D>::sub(y1, y0), x0), RN<D>::mul(RN<D>::sub(x1, x0), y0)));
   s = RN<D>::add(s, RN<D>::sub(RN<D>::mul(RN<D>::sub(y2, y1), x1), RN<D>::mul(RN<D>::sub(x2, x1), y1)));
   s = RN<D>::add(s, RN<D>::sub(RN<D>::mul(RN<D>::sub(y0, y2), x2), RN<D>::mul(RN<D>::sub(x0, x2), y2)));
-  D A = RN<D>::div(s, D(2));
+  D A = RN<D>::mul(s, D(0.5));  // the correctly rounded s / 2, as a division gives
   if (!(dabs(A) < RN<D>::mul(D(10000), factor))) return t;
   D whole = dabs(A);
   if (whole == D(0)) return t;
@@ -421,7 +421,15 @@ __device__ __forceinline__ void deposit_warp_cells(const double2* __restrict__ v
   const long long c = base + lane;
   double2 y0 = make_double2(0, 0), y1 = y0, y2 = y0, y3 = y0;
   if (c < ncells) {
-    long long j = c / ncx, i = c - j * ncx;
+    long long j, i;
+    if (((c | ncx) >> 31) == 0) {  // 32-bit division where it suffices
+      const unsigned jj = unsigned(c) / unsigned(ncx);
+      j = jj;
+      i = unsigned(c) - jj * unsigned(ncx);
+    } else {
+      j = c / ncx;
+      i = c - j * ncx;
+    }
     y0 = verts[((j + 1) * vx + (i + 1)) * vstep];  // z + rhs
     y1 = verts[((j + 1) * vx + i) * vstep];        // z - conj(rhs)
     y2 = verts[(j * vx + i) * vstep];              // z - rhs
@@ -448,9 +456,19 @@ __device__ __forceinline__ void deposit_warp_cells(const double2* __restrict__ v
       h = half == 0 ? setup_head<D>(y0.x, y0.y, y1.x, y1.y, y2.x, y2.y, factor, npx, npy, parities != 0)
                     : setup_head<D>(y2.x, y2.y, y3.x, y3.y, y0.x, y0.y, factor, npx, npy, parities != 0);
     }
-    if (h.single) {
-      const DepositMaps& M = h.map == 0 ? m_total : (h.map == 1 ? m_min : m_sad);
-      atomicAdd(M.acc + (long long)h.oy * npx + h.ox, RN<D>::to_fix(RN<D>::mul(factor, D(kFixScale))));
+    {
+      // lanes in a row whose triangles fall in the same pixel add once for
+      // all of them (adjacent cells of a fine lattice share pixels)
+      unsigned long long* a = nullptr;
+      if (h.single) a = (h.map == 0 ? m_total : (h.map == 1 ? m_min : m_sad)).acc + (long long)h.oy * npx + h.ox;
+      const unsigned long long key = (unsigned long long)a;
+      const unsigned long long prev = __shfl_up_sync(0xffffffffu, key, 1);
+      const unsigned starts = __ballot_sync(0xffffffffu, lane == 0 || prev != key);
+      if (h.single && (starts >> lane & 1u)) {
+        const unsigned later = starts & ~((2u << lane) - 1u);  // lane 31: mask of all bits, none later
+        const int end = later ? __ffs(later) - 1 : 32;
+        atomicAdd(a, (unsigned long long)(end - lane) * RN<D>::to_fix(RN<D>::mul(factor, D(kFixScale))));
+      }
     }
     const bool cx = h.nrows > 0 && !h.single;
     const unsigned b = __ballot_sync(0xffffffffu, cx);
