@@ -6,6 +6,7 @@ interface. Build the libraries with `python -m irs_b200.build`.
 """
 from .adaptive import AdaptiveIPM, LevelNet  # noqa: F401
 from .batch import BatchIPM  # noqa: F401
+from .ccf import CCF  # noqa: F401
 from .mapmaker import IPM, IRS  # noqa: F401
 
-__all__ = ["IPM", "IRS", "BatchIPM", "AdaptiveIPM", "LevelNet"]
+__all__ = ["IPM", "IRS", "BatchIPM", "AdaptiveIPM", "LevelNet", "CCF"]

@@ -3,6 +3,7 @@
 Produces, under irs_b200/lib/:
   lib_ipm.so, lib_ipm_double.so   IPM, float / double (reference lib_ipm.so ABI)
   lib_irs.so, lib_irs_double.so   IRS, float / double (same conventions)
+  lib_ccf.so                      critical curves, double (reference lib_ccf.so ABI)
 and under irs_b200/bin/ the command-line tools of the reference
 (src/main_ipm_irs.cu): ipm_gpu, ipm_gpu_double, irs_gpu, irs_gpu_double.
 
@@ -66,13 +67,13 @@ def _stale(target: str) -> bool:
     return any(os.path.getmtime(s) > t for s in _sources())
 
 
-def build_one(name: str, defs, force: bool = False, extra=None) -> str:
+def build_one(name: str, defs, force: bool = False, extra=None, source: str = "capi.cu") -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     out = os.path.join(LIBDIR, name)
     if not force and not _stale(out):
         return out
     cmd = [nvcc()] + NVCC_FLAGS + list(defs) + list(extra or []) + [
-        "-I", CSRC, os.path.join(CSRC, "capi.cu"), "-o", out + ".tmp", "-lcurand"]
+        "-I", CSRC, os.path.join(CSRC, source), "-o", out + ".tmp", "-lcurand"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
@@ -100,6 +101,7 @@ def build_exe(name: str, defs, force: bool = False) -> str:
 def build(force: bool = False, jobs: int = 4, extra=None, executables: bool = True) -> list[str]:
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
         futs = [ex.submit(build_one, n, d, force, extra) for n, d in VARIANTS.items()]
+        futs.append(ex.submit(build_one, "lib_ccf.so", [], force, extra, "ccf_capi.cu"))
         if executables:
             futs += [ex.submit(build_exe, n, d, force) for n, d in EXECUTABLES.items()]
         return [f.result() for f in cf.as_completed(futs)]

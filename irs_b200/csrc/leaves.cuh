@@ -25,6 +25,30 @@
 
 namespace irsb {
 
+// Tree nodes needed by the descent, and the node -> leaf map. The descent is
+// get_nearest_node (tree_node.cuh:529-561) for points inside the root box.
+template <typename T>
+struct DescentPtrs {
+  const T* cx;
+  const T* cy;
+  const int* child0;
+  const long long* leaf_of_node;  // exclusive scan of the leaf flags
+  const int* tile_leaf;           // per tile: the leaf owning all its points, or -1 (nullptr: not known)
+};
+
+template <typename T>
+__device__ __forceinline__ int descend_leaf(const DescentPtrs<T>& d, double x, double y) {
+  int k = 0;
+  for (int it = 0; it < kMaxLevels + 1; it++) {
+    const int c0 = d.child0[k];
+    if (c0 < 0) break;
+    const double cx = double(d.cx[k]), cy = double(d.cy[k]);
+    const bool right = x >= cx, top = y >= cy;
+    k = c0 + (right ? (top ? 0 : 3) : (top ? 1 : 2));
+  }
+  return int(d.leaf_of_node[k]);
+}
+
 constexpr int kTileX = 32;
 constexpr int kTileY = 32;
 

@@ -3,6 +3,7 @@
 //   alpha_smooth           :62-127  (rectangular/circular x approximate/exact)
 //   d_alpha_smooth_d_z     :141-170
 //   d_alpha_smooth_d_zbar  :185-236
+//   d2_alpha_smooth_d_zbar2 :251-300
 // The rectangular approximate form is the degree-`taylor_smooth` series in
 // conj(z)/corner of the exact four-logarithm expression.
 #pragma once
@@ -98,6 +99,36 @@ IRSB_HD cplx<T> d_alpha_smooth_dzbar_(cplx<T> z, T ks, int rect, cplx<T> c, int 
     T ca = cabs_(c);
     cplx<T> zb = cconj(z);
     d = cdiv(mk<T>(ks * ca * ca, 0), cmul(zb, zb));
+  }
+  return d;
+}
+
+template <typename T>
+IRSB_HD cplx<T> d2_alpha_smooth_dzbar2_(cplx<T> z, T ks, int rect, cplx<T> c, int approx, int ts, T inv_pi) {
+  cplx<T> d = mk<T>(0, 0);
+  cplx<T> zb = cconj(z);
+  if (rect) {
+    if (approx) {
+      cplx<T> r = cdiv(zb, c);
+      cplx<T> r2 = cmul(r, r);
+      T ph = carg(c);
+      for (int i = ts - 1; i >= 2; i -= 2) {
+        cplx<T> e = cexp_(mk<T>(0, 2 * ph * i));
+        d = cadd(d, mk<T>(1 - e.re, -e.im));
+        d = cmul(d, r2);
+      }
+      d = cdiv(d, zb);
+      d = cscale(d, T(2));
+      d = cmul(d, mk<T>(0, -ks * inv_pi));
+    } else {
+      cplx<T> c1 = csub(cconj(c), zb), c2 = csub(c, zb), c3 = csub(cneg(c), zb), c4 = csub(cneg(cconj(c)), zb);
+      cplx<T> one = mk<T>(1, 0);
+      d = cadd(csub(cadd(cneg(cdiv(one, c1)), cdiv(one, c2)), cdiv(one, c4)), cdiv(one, c3));
+      d = cmul(d, mk<T>(0, -ks * inv_pi));
+    }
+  } else if (!approx) {
+    T ca = cabs_(c);
+    d = cdiv(mk<T>(-2 * ks * ca * ca, 0), cmul(cmul(zb, zb), zb));
   }
   return d;
 }

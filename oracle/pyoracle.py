@@ -214,7 +214,9 @@ def ref_lib(kind="ipm"):
             getattr(L, f).restype = i
         L.ref_tree_nodes.argtypes = [vp] + [vp] * 7
         L.ref_points.argtypes = [vp, C.POINTER(RefLens), ll, vp, vp, vp, vp, i]
-        if kind == "ipm":
+        if kind == "ccf":
+            L.ref_ccf_run.argtypes = [vp, C.POINTER(RefLens), i, i, i, vp, i, i, vp, vp, vp, vp]
+        elif kind == "ipm":
             L.ref_shoot_cells.argtypes = [vp, C.POINTER(RefLens), d, d, i, i, d, d, d, d, d, d, d, d, i, i, vp, vp,
                                           vp, i]
             L.ref_deposit_cells.argtypes = [ll, ll, vp, d, i, i, vp, vp, vp, i]
@@ -289,3 +291,26 @@ def ref_deposit_cells(verts, factor, npix, parities=False):
     L.ref_deposit_cells(ncx, ncy, _p(v), float(factor), npix[0], npix[1], _p(pix), _p(pmin), _p(psad),
                         int(parities))
     return (pmin + psad, pmin, psad) if parities else pix
+
+
+def ref_ccf_available() -> bool:
+    return os.path.exists(os.path.join(REFDIR, "libref_ccf.so"))
+
+
+def ref_ccf(stars, lens_, root_hl, init_roots, nphi, nb, iters=(30, 20), alpha_error=1e-7):
+    """The reference's own critical-curve pipeline (include/ccf.cuh) on the
+    host: tree and expansions of `stars` (x, y, m rows, in the given order),
+    then the root finding from `init_roots` ((nphi + nb, nroots) complex, the
+    branch-centre rows filled). Returns (ccs, caustics, mu_length_scales,
+    max_error) with ccs / caustics of shape (nroots * nb, nphi / nb + 1)."""
+    tree = RefTree(stars, root_hl, 0, lens_.theta, alpha_error * lens_.theta, kind="ccf")
+    z = np.ascontiguousarray(np.asarray(init_roots, np.complex128))
+    rows, nroots = z.shape
+    ccs = np.zeros(rows * nroots, np.complex128)
+    caus = np.zeros_like(ccs)
+    mu = np.zeros(rows * nroots)
+    me = C.c_double(0)
+    tree.L.ref_ccf_run(tree.h, C.byref(ref_lens(lens_)), nroots, int(nphi), int(nb), _p(z), int(iters[0]),
+                       int(iters[1]), _p(ccs), _p(caus), _p(mu), C.byref(me))
+    shape = (nroots * nb, nphi // nb + 1)
+    return ccs.reshape(shape), caus.reshape(shape), mu.reshape(shape), me.value, tree

@@ -6,6 +6,7 @@
 // outputs go to oracle/_ref/. Two libraries are built from this file:
 //   -DREF_IPM -> libref_ipm.so  (ipm_functions.cuh: shoot_cells_kernel)
 //   -DREF_IRS -> libref_irs.so  (irs_functions.cuh: shoot_rays_kernel)
+//   -DREF_CCF -> libref_ccf.so  (ccf_functions.cuh: the critical-curve kernels)
 // (the two headers define the same lens-equation templates, so they cannot
 // share a translation unit).
 //
@@ -30,8 +31,11 @@
 #include "ipm_functions.cuh"
 #elif defined(REF_IRS)
 #include "irs_functions.cuh"
+#elif defined(REF_CCF)
+#include "array_functions.cuh"
+#include "ccf_functions.cuh"
 #else
-#error "define REF_IPM or REF_IRS"
+#error "define REF_IPM, REF_IRS or REF_CCF"
 #endif
 
 thread_local shim_uint3 threadIdx, blockIdx;
@@ -275,6 +279,56 @@ void ref_shoot_rays(RefTree* r, const RefLens* L, double rhs1, double rhs2, int 
                          Complex<T>(hly1, hly2), pmin, psad, pixels, Complex<int>(npx, npy), &percentage, 0);
   }
   serial_grid();
+}
+#endif
+
+#if defined(REF_CCF)
+// The root finding of include/ccf.cuh (find_initial_roots :906-977 and
+// find_ccs :979-1083) with the reference's own kernels, the grid emulated by
+// one host thread (its loops visit branch, side, root in order), followed by
+// find_caustics_kernel and find_mu_length_scales_kernel (:1085-1121).
+// roots: (nphi + nb) x nroots complex values, the branch centre rows holding
+// the initial roots; on return every row holds its roots. ccs / caustics /
+// mu_len: outputs in the [root][row] layout; *max_error: the largest error in
+// 1/mu (negative when one is not finite).
+void ref_ccf_run(RefTree* r, const RefLens* L, int nroots, int nphi, int nb, double* roots, int iters_init,
+                 int iters_step, double* ccs, double* caustics, double* mu_len, double* max_error) {
+  serial_grid();
+  const int rows = nphi + nb;
+  Complex<T>* z = reinterpret_cast<Complex<T>*>(roots);
+  bool* fin = new bool[(size_t)nb * 2 * nroots]();
+  T* errs = new T[(size_t)rows * nroots];
+  const Complex<T> corner(L->corner_re, L->corner_im);
+  for (int i = 0; i < iters_init; i++)
+    find_critical_curve_roots_kernel<T>(L->kappa, L->gamma, L->theta, r->stars, L->kstar, r->tree[0], L->rect, corner,
+                                        L->approx, L->taylor_smooth, z, nroots, 0, nphi, nb, fin);
+  for (int j = 1; j <= nphi / (2 * nb); j++) {
+    prepare_roots_kernel<T>(z, nroots, j, nphi, nb, fin);
+    for (int i = 0; i < iters_step; i++)
+      find_critical_curve_roots_kernel<T>(L->kappa, L->gamma, L->theta, r->stars, L->kstar, r->tree[0], L->rect,
+                                          corner, L->approx, L->taylor_smooth, z, nroots, j, nphi, nb, fin);
+  }
+  for (long long q = 0; q < (long long)rows * nroots; q++) errs[q] = 1;
+  for (int j = 0; j <= nphi / (2 * nb); j++)
+    find_errors_kernel<T>(z, nroots, L->kappa, L->gamma, L->theta, r->stars, L->kstar, r->tree[0], L->rect, corner,
+                          L->approx, L->taylor_smooth, j, nphi, nb, errs);
+  double me = 0;
+  for (long long q = 0; q < (long long)rows * nroots; q++) {
+    if (!std::isfinite(errs[q])) {
+      me = -1;
+      break;
+    }
+    me = std::max(me, double(errs[q]));
+  }
+  *max_error = me;
+  Complex<T>* out = reinterpret_cast<Complex<T>*>(ccs);
+  transpose_array_kernel<Complex<T>>(z, rows, nroots, out);
+  find_caustics_kernel<T>(out, rows * nroots, L->kappa, L->gamma, L->theta, r->stars, L->kstar, r->tree[0], L->rect,
+                          corner, L->approx, L->taylor_smooth, reinterpret_cast<Complex<T>*>(caustics));
+  find_mu_length_scales_kernel<T>(out, rows * nroots, L->kappa, L->gamma, L->theta, r->stars, L->kstar, r->tree[0],
+                                  L->rect, corner, L->approx, L->taylor_smooth, mu_len);
+  delete[] fin;
+  delete[] errs;
 }
 #endif
 

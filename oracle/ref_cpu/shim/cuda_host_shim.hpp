@@ -81,6 +81,10 @@ inline T atomicMin(T* a, U v) {
   return old;
 }
 template <typename T, typename U>
+inline T atomicExch(T* a, U v) {
+  return std::atomic_ref<T>(*a).exchange(static_cast<T>(v));
+}
+template <typename T, typename U>
 inline T atomicMax(T* a, U v) {
   std::atomic_ref<T> r(*a);
   T old = r.load();
