@@ -371,6 +371,91 @@ def adaptive_measure():
     return res
 
 
+CCF_CASES = (137, 1000, 4000)  # stars; kappa_tot 0.3, shear 0.3, kappa_star 0.27 (the reference CCF defaults)
+
+
+def ccf_stars(n, seed=7, kstar=0.27):
+    """Seeded equal-mass circular field of n stars and its radius (the reference's
+    CCF field size for n stars, include/ccf.cuh:427-432)."""
+    rng = np.random.default_rng(seed)
+    rad = np.sqrt(n / kstar)
+    r = rad * np.sqrt(rng.random(n))
+    a = 2 * np.pi * rng.random(n)
+    return np.stack([r * np.cos(a), r * np.sin(a), np.ones(n)], 1), rad
+
+
+def ccf_write_stars(path, stars, rad):
+    with open(path, "wb") as f:
+        f.write(np.array([len(stars), 0], np.int32).tobytes())
+        f.write(np.array([rad, 0.0, 1.0]).tobytes())
+        f.write(np.ascontiguousarray(stars, np.float64).tobytes())
+
+
+def ccf_measure():
+    """Critical curves (CCF, 100 phi steps, one branch) of seeded equal-mass
+    fields: device time of the root finding (branch centres + phi steps), the
+    critical-curve points found per second, the largest error in 1/mu."""
+    import tempfile
+
+    import irs_b200
+    res = {}
+    with tempfile.TemporaryDirectory() as td:
+        for n in CCF_CASES:
+            stars, rad = ccf_stars(n)
+            sf = os.path.join(td, f"s{n}.bin")
+            ccf_write_stars(sf, stars, rad)
+            c = irs_b200.CCF(kappa_tot=0.3, shear=0.3, starfile=sf, num_phi=100, write_caustics=True)
+            c.run()
+            c.run()  # warm
+            t = c.value("t_init_roots") + c.t_ccs
+            pts = c.num_roots * 101
+            res[f"stars_{n}"] = {"roots": c.num_roots, "points": pts, "root_finding_ms": t * 1e3,
+                                 "caustics_ms": c.value("t_caustics") * 1e3, "points_per_s": pts / t,
+                                 "max_error_inv_mu": c.value("max_error"),
+                                 "expansion_order": int(c.value("expansion_order"))}
+            c.close()
+    return res
+
+
+def ccf_cpu_reference(gpu_res, cases=(137, 400)):
+    """The reference's own CCF (include/ccf.cuh, compiled for the host; its
+    kernels on one host thread) on the same fields, and the GPU's curves
+    against it (the two update schemes label the roots differently: matched
+    at the branch centre)."""
+    import tempfile
+
+    from scipy.optimize import linear_sum_assignment
+
+    import irs_b200
+    from oracle import ccf_ref, pyoracle as po
+    if not po.ref_ccf_available():
+        return {"unavailable": "oracle/_ref/libref_ccf.so not built"}
+    out = {}
+    with tempfile.TemporaryDirectory() as td:
+        for n in cases:
+            stars, rad = ccf_stars(n)
+            init = ccf_ref.initial_roots(stars, 2 * n, 100, 1, rad)
+            lens = po.lens(0.3, 0.3, float(np.sum(stars[:, 2]) / rad ** 2), 1.0, 0, 1, 1, (rad, 0.0))
+            t0 = time.perf_counter()
+            rc, _, _, rme, _ = po.ref_ccf(stars, lens, rad * 1.1, init, 100, 1)
+            t_cpu = time.perf_counter() - t0
+            sf = os.path.join(td, f"s{n}.bin")
+            ccf_write_stars(sf, stars, rad)
+            c = irs_b200.CCF(kappa_tot=0.3, shear=0.3, starfile=sf, num_phi=100, write_caustics=False)
+            c.run()
+            g = c.critical_curves[..., 0] + 1j * c.critical_curves[..., 1]
+            t_gpu = c.value("t_init_roots") + c.t_ccs
+            c.close()
+            d = np.abs(rc[:, 50][:, None] - g[:, 50][None, :])
+            i, j = linear_sum_assignment(d)
+            perm = np.empty_like(j)
+            perm[i] = j
+            out[f"stars_{n}"] = {"seconds": t_cpu, "cores": 1, "max_error_inv_mu": rme,
+                                 "gpu_seconds": t_gpu, "speedup": t_cpu / t_gpu,
+                                 "max_curve_deviation": float(np.abs(rc - g[perm]).max())}
+    return out
+
+
 def our_arm(args):
     import torch
 
@@ -507,9 +592,12 @@ def our_arm(args):
         gb.close()
         extra["batched_256"] = batch_measure(args.steps)
         extra["learned_adaptive"] = adaptive_measure()
+        extra["ccf"] = ccf_measure()
 
     if rank == 0:
         cpu = cpu_baseline(m, stars.astype(np.float64), os.cpu_count() or 1) if (ws == 1 and not args.no_cpu) else None
+        if cpu is not None and not args.no_extra:
+            cpu["ccf_reference"] = ccf_cpu_reference(extra.get("ccf"))
         out = {
             "metric": "IPM pixels/s", "value": value, "unit": "pixels/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_time / args.steps * 1e3, "higher_is_better": True,

@@ -15,10 +15,10 @@
 // mu_length_scale (:145-166).
 //
 // How, differently by design:
-//   * one thread per (chain, root), a chain being one side of one branch; the
-//     O(N) sums over all stars and over the chain's roots are tiled through
-//     shared memory (every CTA stages 256 positions at a time and each thread
-//     reads them as broadcasts), FP64 throughout;
+//   * one warp per (chain, root), a chain being one side of one branch: the
+//     lanes split the near-field stars and the O(N) sums over all stars and
+//     over the chain's roots, then reduce them in a fixed order; FP64
+//     throughout;
 //   * the update is a Jacobi step (all roots read the previous iterate from
 //     one buffer and write the next to another) instead of the reference's
 //     in-place update, whose result depends on thread timing; the roots, their
@@ -27,7 +27,7 @@
 //     the lens-equation kernels (near64, coef64 = k c_k); a point outside the
 //     root box takes the direct sum over all stars, as get_nearest_node
 //     returns the root there (tree_node.cuh:535-539);
-//   * a CTA whose roots are all final skips the sums.
+//   * a final root costs its warp one load and one store.
 #pragma once
 #include "leaves.cuh"
 #include "shoot.cuh"  // LeafPtrs
@@ -145,72 +145,106 @@ __device__ __forceinline__ cplx<double> recip(cplx<double> d) {
   return mk(d.re * inv, -d.im * inv);
 }
 
+__device__ __forceinline__ cplx<double> warp_sum(cplx<double> v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v.re += __shfl_xor_sync(0xffffffffu, v.re, o);
+    v.im += __shfl_xor_sync(0xffffffffu, v.im, o);
+  }
+  return v;
+}
+
+// ccf_field with the work of one root spread over a warp: lane l takes the
+// near-field stars l, l + 32, ... (one each for a leaf's <= 32) and the
+// partial sums meet in a butterfly reduction (fixed order: deterministic);
+// every lane then evaluates the local expansion (the same dz) itself.
+template <typename T>
+__device__ __forceinline__ CcfField ccf_field_warp(const CcfParams& P, const LeafPtrs& lp, const DescentPtrs<T>& dp,
+                                                   const StarRec<T>* __restrict__ stars, cplx<double> z, int lane) {
+  CcfField f;
+  f.s1 = f.s2 = f.s3 = f.a0 = f.a1 = f.a2 = mk(0.0, 0.0);
+  f.hl = 1.0;
+  const bool outside = fabs(z.re) > P.root_hl || fabs(z.im) > P.root_hl;
+  int leaf = 0;
+  if (outside) {  // the root node: every star, no expansion
+    for (int i = lane; i < P.nstars; i += 32) ccf_add_star(f, z, double(stars[i].x), double(stars[i].y), double(stars[i].m));
+  } else {
+    leaf = descend_leaf(dp, z.re, z.im);
+    const int nn = lp.nnear[leaf];
+    if (lane < nn) {
+      const double4 st = lp.near64[(size_t)leaf * kMaxStarsDirect + lane];
+      ccf_add_star(f, z, st.x, st.y, st.z);
+    }
+  }
+  f.s1 = warp_sum(f.s1);
+  f.s2 = warp_sum(f.s2);
+  f.s3 = warp_sum(f.s3);
+  if (outside) return f;
+  f.hl = lp.hl[leaf];
+  const cplx<double> dz = mk((z.re - lp.cx[leaf]) / f.hl, (z.im - lp.cy[leaf]) / f.hl);
+  const double2* coef = lp.coef64 + (size_t)leaf * kMaxOrder;
+  for (int k = P.p; k >= 1; k--) {
+    const double2 c = coef[k - 1];  // k c_k
+    f.a0 = cadd(cmul(f.a0, dz), mk(c.x, c.y));
+    if (k >= 2) f.a1 = cadd(cmul(f.a1, dz), mk(c.x * (k - 1), c.y * (k - 1)));
+    if (k >= 3) f.a2 = cadd(cmul(f.a2, dz), mk(c.x * ((k - 1) * (k - 2)), c.y * ((k - 1) * (k - 2))));
+  }
+  return f;
+}
+
 // One Jacobi step for chains [0, nchains): chain ch is branch ch / sides,
 // side (ch % sides) (0: phi decreasing, 1: increasing; sides = 1 at j = 0,
 // where both sides start from the branch centre). Positions are read from
 // `src` (rows of the root array, or the chain's scratch row) and written to
-// `dst`; fin[ch][a] marks final roots, which are copied.
+// `dst`; fin[ch][a] marks final roots, which are copied. One warp per root:
+// the lanes split the sums over all stars and over the chain's other roots
+// (strided, so a warp reads 32 consecutive positions at a time; the star and
+// root arrays stay in L1) and reduce them in a fixed order.
 template <typename T>
 __global__ void __launch_bounds__(kCcfThreads) ccf_iterate(CcfParams P, LeafPtrs lp, DescentPtrs<T> dp,
                                                            const StarRec<T>* __restrict__ stars, int j, int sides,
                                                            int from_scratch, double2* __restrict__ roots,
                                                            double2* __restrict__ scratch,
                                                            unsigned char* __restrict__ fin) {
-  __shared__ double2 tile[kCcfThreads];
+  const int lane = threadIdx.x & 31;
   const int ch = blockIdx.y;
   const int c = ch / sides, side = ch % sides;
   const int sj = side == 0 ? -j : j;
-  const int a = blockIdx.x * kCcfThreads + threadIdx.x;
+  const int a = blockIdx.x * (kCcfThreads / 32) + (threadIdx.x >> 5);  // root of this warp
+  if (a >= P.nroots) return;                                           // whole warps only
   const double2* src = from_scratch ? scratch + (size_t)ch * P.nroots : roots + (size_t)ccf_row(P, c, sj) * P.nroots;
   double2* dst = from_scratch ? roots + (size_t)ccf_row(P, c, sj) * P.nroots : scratch + (size_t)ch * P.nroots;
   unsigned char* fn = fin + (size_t)ch * P.nroots;
-  const bool mine = a < P.nroots;
-  const cplx<double> z = mine ? mk(src[a].x, src[a].y) : mk(0.0, 0.0);
-  bool active = mine && !fn[a];
-  cplx<double> f0 = mk(0.0, 0.0), f1 = f0;
-  if (active) {
-    const CcfField f = ccf_field(P, lp, dp, stars, z);
-    const CcfDerivs d = ccf_derivs(P, f, z);
-    f0 = ccf_f0(d, ccf_phi(P, c, sj));
-    if (ccf_inv_mu_bound(cabs_(f0), d.dwdz) < 1e-9) {
-      active = false;  // already a root to the precision sought: stays, and is final
-      fn[a] = 1;
-    }
-    f1 = d.d2wdzb2;
-    f1 = cconj(f1);  // f1 = d f0 / dz = -conj(d2 alpha / d zbar2) summed = conj(d2w/dzbar2)
-  }
-  // the CTA skips the sums when none of its roots moves
-  if (!__syncthreads_or(active)) {
-    if (mine) dst[a] = src[a];
+  const double2 z2 = src[a];
+  const cplx<double> z = mk(z2.x, z2.y);
+  if (fn[a]) {
+    if (lane == 0) dst[a] = z2;
     return;
   }
-  cplx<double> ps = mk(0.0, 0.0), rs = mk(0.0, 0.0);
-  for (int t0 = 0; t0 < P.nstars; t0 += kCcfThreads) {
-    const int i = t0 + threadIdx.x;
-    if (i < P.nstars) tile[threadIdx.x] = make_double2(double(stars[i].x), double(stars[i].y));
-    __syncthreads();
-    const int nt = min(kCcfThreads, P.nstars - t0);
-    if (active)
-      for (int k = 0; k < nt; k++) ps = cadd(ps, recip(mk(z.re - tile[k].x, z.im - tile[k].y)));
-    __syncthreads();
+  const CcfField f = ccf_field_warp(P, lp, dp, stars, z, lane);
+  const CcfDerivs d = ccf_derivs(P, f, z);
+  const cplx<double> f0 = ccf_f0(d, ccf_phi(P, c, sj));
+  if (ccf_inv_mu_bound(cabs_(f0), d.dwdz) < 1e-9) {  // already a root to the precision sought: final
+    __syncwarp();
+    if (lane == 0) {
+      fn[a] = 1;
+      dst[a] = z2;
+    }
+    return;
   }
+  const cplx<double> f1 = cconj(d.d2wdzb2);  // d f0 / dz
+  cplx<double> ps = mk(0.0, 0.0), rs = mk(0.0, 0.0);
+  for (int i = lane; i < P.nstars; i += 32) ps = cadd(ps, recip(mk(z.re - double(stars[i].x), z.im - double(stars[i].y))));
+  for (int i = lane; i < P.nroots; i += 32)
+    if (i != a) {
+      const double2 w = src[i];
+      rs = cadd(rs, recip(mk(z.re - w.x, z.im - w.y)));
+    }
+  ps = warp_sum(ps);
+  rs = warp_sum(rs);
+  if (lane != 0) return;
   if (!P.rect && !P.approx) ps = cadd(ps, recip(z));
   ps = cscale(ps, 2.0);
-  for (int t0 = 0; t0 < P.nroots; t0 += kCcfThreads) {
-    const int i = t0 + threadIdx.x;
-    if (i < P.nroots) tile[threadIdx.x] = src[i];
-    __syncthreads();
-    const int nt = min(kCcfThreads, P.nroots - t0);
-    if (active)
-      for (int k = 0; k < nt; k++)
-        if (t0 + k != a) rs = cadd(rs, recip(mk(z.re - tile[k].x, z.im - tile[k].y)));
-    __syncthreads();
-  }
-  if (!mine) return;
-  if (!active) {
-    dst[a] = src[a];
-    return;
-  }
   const cplx<double> den = cadd(f1, cmul(f0, csub(ps, rs)));
   const cplx<double> zn = csub(z, cdiv(f0, den));
   if (cabs_(csub(zn, z)) / sqrt(P.theta2) < 1e-9) fn[a] = 1;

@@ -226,7 +226,8 @@ class CCF {
     IRSB_CKR(cudaMemsetAsync(d_fin_.p, 0, (size_t)nch * num_roots, s));
     const LeafPtrs lp = leaf_ptrs();
     const DescentPtrs<T> dp{tree_.cx.p, tree_.cy.p, tree_.child0.p, leaves_.pos.p, nullptr};
-    const dim3 g0(ceil_div(num_roots, kCcfThreads), num_branches), g1(ceil_div(num_roots, kCcfThreads), nch);
+    const int rpb = kCcfThreads / 32;  // roots per CTA (a warp each)
+    const dim3 g0(ceil_div(num_roots, rpb), num_branches), g1(ceil_div(num_roots, rpb), nch);
     const int it0 = num_iters_init + (num_iters_init & 1), it1 = num_iters_step + (num_iters_step & 1);
     IRSB_CKR(cudaEventRecord(e0_, s));
     for (int i = 0; i < it0; i++) {  // branch centres (include/ccf.cuh:906-977)
