@@ -8,5 +8,6 @@ from .adaptive import AdaptiveIPM, LevelNet  # noqa: F401
 from .batch import BatchIPM  # noqa: F401
 from .ccf import CCF  # noqa: F401
 from .mapmaker import IPM, IRS  # noqa: F401
+from .ncc import NCC  # noqa: F401
 
-__all__ = ["IPM", "IRS", "BatchIPM", "AdaptiveIPM", "LevelNet", "CCF"]
+__all__ = ["IPM", "IRS", "BatchIPM", "AdaptiveIPM", "LevelNet", "CCF", "NCC"]

@@ -4,6 +4,7 @@ Produces, under irs_b200/lib/:
   lib_ipm.so, lib_ipm_double.so   IPM, float / double (reference lib_ipm.so ABI)
   lib_irs.so, lib_irs_double.so   IRS, float / double (same conventions)
   lib_ccf.so                      critical curves, double (reference lib_ccf.so ABI)
+  lib_ncc.so                      caustic-crossing maps, double (reference lib_ncc.so ABI)
 and under irs_b200/bin/ the command-line tools of the reference
 (src/main_ipm_irs.cu): ipm_gpu, ipm_gpu_double, irs_gpu, irs_gpu_double.
 
@@ -102,6 +103,7 @@ def build(force: bool = False, jobs: int = 4, extra=None, executables: bool = Tr
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
         futs = [ex.submit(build_one, n, d, force, extra) for n, d in VARIANTS.items()]
         futs.append(ex.submit(build_one, "lib_ccf.so", [], force, extra, "ccf_capi.cu"))
+        futs.append(ex.submit(build_one, "lib_ncc.so", [], force, extra, "ncc_capi.cu"))
         if executables:
             futs += [ex.submit(build_exe, n, d, force) for n, d in EXECUTABLES.items()]
         return [f.result() for f in cf.as_completed(futs)]

@@ -1034,3 +1034,99 @@ void orc_derive(double kappa, double gamma, double kstar, double theta, double m
   double v[14] = {mu_ave, nrx, r1, r2, h1, h2, 2.0 * n1, 2.0 * n2, c1, c2, (double)ns, k1, k2, ae};
   memcpy(out, v, sizeof(v));
 }
+
+/* ---------------------------------------------------------------- NCC
+ * Number of caustic crossings (include/ncc_functions.cuh:149-367 and
+ * include/ncc.cuh:208-327), restated: the same clipping of every caustic
+ * segment into the region y1 > -hl1, |y2| < hl2, the same pixel-centre row
+ * crossings adding -1 (segment going up) or +1 (going down) to every pixel of
+ * the row left of the crossing, on the 2^os times finer map, then the maximum
+ * over 2^os x 2^os blocks. The intersection of a segment with a horizontal or
+ * vertical line is x0 + ((y - y0) / dy) dx, each operation rounded (the
+ * reference evaluates it through logarithms), as the GPU kernels
+ * (irs_b200/csrc/ncc.cuh) compute it. out: npy x npx int32, row 0 at the top. */
+static double ncc_sgn(double v) { return v < 0 ? -1.0 : (v > 0 ? 1.0 : 0.0); }
+static double ncc_x_at(double y, double x0, double y0, double x1, double y1) {
+  double dx = x1 - x0;
+  if (dx == 0.0) return x0;
+  double dy = y1 - y0, t = y - y0;
+  t = t / dy;
+  t = t * dx;
+  return x0 + t;
+}
+static double ncc_y_at(double x, double x0, double y0, double x1, double y1) {
+  double dy = y1 - y0;
+  if (dy == 0.0) return y0;
+  double dx = x1 - x0, t = x - x0;
+  t = t / dx;
+  t = t * dy;
+  return y0 + t;
+}
+static void ncc_correct(double* x, double* y, double xo, double yo, double hl1, double hl2, int fx, int fy) {
+  double x0 = *x, y0 = *y;
+  if (*x <= -hl1) {
+    double d = 0.01 * 2;
+    d = d * hl1;
+    d = d / (double)fx;
+    *x = -hl1 + d;
+    *y = ncc_y_at(*x, x0, y0, xo, yo);
+  }
+  if (fabs(*y) >= hl2) {
+    double d = 0.01 * 2;
+    d = d * hl2;
+    d = d / (double)fy;
+    d = hl2 - d;
+    *y = ncc_sgn(*y) * d;
+    *x = ncc_x_at(*y, x0, y0, xo, yo);
+  }
+}
+
+int orc_ncc(const double* caus, int nrows, int ncols, double cy1, double cy2, double hl1, double hl2, int npx, int npy,
+            int os, int* out) {
+  int B = 1 << os, fx = npx * B, fy = npy * B, errors = 0;
+  int* fine = (int*)calloc((size_t)fx * fy, sizeof(int));
+  for (long long i = 0; i < nrows; i++)
+    for (long long j = 0; j + 1 < ncols; j++) {
+      const double* a = caus + 2 * (i * ncols + j);
+      const double* b = a + 2;
+      double x0 = a[0] - cy1, y0 = a[1] - cy2, x1 = b[0] - cy1, y1 = b[1] - cy2;
+      int use = (x0 > -hl1 && fabs(y0) < hl2) || (x1 > -hl1 && fabs(y1) < hl2);
+      if (!use)
+        use = ncc_x_at(hl2, x0, y0, x1, y1) >= -hl1 || ncc_x_at(-hl2, x0, y0, x1, y1) >= -hl1 ||
+              fabs(ncc_y_at(-hl1, x0, y0, x1, y1)) <= hl2;
+      if (!use) continue;
+      ncc_correct(&x0, &y0, x1, y1, hl1, hl2, fx, fy);
+      ncc_correct(&x1, &y1, x0, y0, hl1, hl2, fx, fy);
+      double s1 = 2 * hl1, s2 = 2 * hl2, t;
+      t = x0 + hl1; t = t * (double)fx; double px0 = t / s1;
+      t = y0 + hl2; t = t * (double)fy; double py0 = t / s2;
+      t = x1 + hl1; t = t * (double)fx; double px1 = t / s1;
+      t = y1 + hl2; t = t * (double)fy; double py1 = t / s2;
+      if (py0 == py1) continue;
+      int up = py0 < py1, k0 = (int)(py0 + 0.5), k1 = (int)(py1 + 0.5), v = up ? -1 : 1;
+      for (int k = k0; up ? k < k1 : k > k1; k += up ? 1 : -1) {
+        double yc = up ? (double)k + 0.5 : (double)k - 0.5;
+        double xc = ncc_x_at(yc, px0, py0, px1, py1);
+        int col = (int)(xc + 0.5) - 1, row = fy - 1 - (up ? k : k - 1);
+        if (col > fx - 1) col = fx - 1;
+        if (col < 0) continue;
+        if (row < 0 || row >= fy) { /* the reference reports it and adds nothing */
+          errors++;
+          continue;
+        }
+        for (int l = 0; l <= col; l++) fine[(long long)row * fx + l] += v;
+      }
+    }
+  for (int r = 0; r < npy; r++)
+    for (int c = 0; c < npx; c++) {
+      int m = fine[(long long)r * B * fx + (long long)c * B];
+      for (int dy = 0; dy < B; dy++)
+        for (int dx = 0; dx < B; dx++) {
+          int q = fine[((long long)r * B + dy) * fx + (long long)c * B + dx];
+          m = q > m ? q : m;
+        }
+      out[(long long)r * npx + c] = m;
+    }
+  free(fine);
+  return errors;
+}

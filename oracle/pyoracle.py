@@ -52,6 +52,8 @@ def lib():
         L.orc_ipm_deposit_fix_f32.argtypes = [ll, ll, vp, C.c_float, i, i, vp, vp, vp, i]
         L.orc_ipm_deposit_fix_f64.argtypes = [ll, ll, vp, d, i, i, vp, vp, vp, i]
         L.orc_derive.argtypes = [d, d, d, d, d, d, d, i, d, d, d, d, d, i, i, i, vp]
+        L.orc_ncc.argtypes = [vp, i, i, d, d, d, d, i, i, i, vp]
+        L.orc_ncc.restype = i
         _lib = L
     return _lib
 
@@ -206,6 +208,10 @@ def ref_lib(kind="ipm"):
     if kind not in _ref:
         L = C.CDLL(os.path.join(REFDIR, f"libref_{kind}.so"))
         vp, d, i, ll = C.c_void_p, C.c_double, C.c_int, C.c_longlong
+        if kind == "ncc":
+            L.ref_ncc_run.argtypes = [vp, i, i, d, d, d, d, i, i, i, vp]
+            _ref[kind] = L
+            return L
         L.ref_tree_build.argtypes = [i, vp, d, i, d, d]
         L.ref_tree_build.restype = vp
         L.ref_tree_free.argtypes = [vp]
@@ -314,3 +320,28 @@ def ref_ccf(stars, lens_, root_hl, init_roots, nphi, nb, iters=(30, 20), alpha_e
                        int(iters[1]), _p(ccs), _p(caus), _p(mu), C.byref(me))
     shape = (nroots * nb, nphi // nb + 1)
     return ccs.reshape(shape), caus.reshape(shape), mu.reshape(shape), me.value, tree
+
+
+def ncc(caustics, center, half_length, npix, over_sample=2):
+    """Number-of-caustic-crossings map (oracle restatement, oracle.c orc_ncc):
+    caustics (rows, cols) complex; returns (npy, npx) int32 and the number of
+    crossings that fell outside the map."""
+    c = np.ascontiguousarray(np.asarray(caustics, np.complex128))
+    out = np.zeros((npix[1], npix[0]), np.int32)
+    err = lib().orc_ncc(_p(c), c.shape[0], c.shape[1], float(center[0]), float(center[1]), float(half_length[0]),
+                        float(half_length[1]), int(npix[0]), int(npix[1]), int(over_sample), _p(out))
+    return out, err
+
+
+def ref_ncc_available() -> bool:
+    return os.path.exists(os.path.join(REFDIR, "libref_ncc.so"))
+
+
+def ref_ncc(caustics, center, half_length, npix, over_sample=2):
+    """The reference's own NCC kernels on the host (oracle/_ref/libref_ncc.so)."""
+    c = np.ascontiguousarray(np.asarray(caustics, np.complex128))
+    out = np.zeros((npix[1], npix[0]), np.int32)
+    ref_lib("ncc").ref_ncc_run(_p(c), c.shape[0], c.shape[1], float(center[0]), float(center[1]),
+                               float(half_length[0]), float(half_length[1]), int(npix[0]), int(npix[1]),
+                               int(over_sample), _p(out))
+    return out

@@ -7,6 +7,7 @@
 //   -DREF_IPM -> libref_ipm.so  (ipm_functions.cuh: shoot_cells_kernel)
 //   -DREF_IRS -> libref_irs.so  (irs_functions.cuh: shoot_rays_kernel)
 //   -DREF_CCF -> libref_ccf.so  (ccf_functions.cuh: the critical-curve kernels)
+//   -DREF_NCC -> libref_ncc.so  (ncc_functions.cuh: the caustic-crossing kernels)
 // (the two headers define the same lens-equation templates, so they cannot
 // share a translation unit).
 //
@@ -34,8 +35,10 @@
 #elif defined(REF_CCF)
 #include "array_functions.cuh"
 #include "ccf_functions.cuh"
+#elif defined(REF_NCC)
+#include "ncc_functions.cuh"
 #else
-#error "define REF_IPM, REF_IRS or REF_CCF"
+#error "define REF_IPM, REF_IRS, REF_CCF or REF_NCC"
 #endif
 
 thread_local shim_uint3 threadIdx, blockIdx;
@@ -188,6 +191,7 @@ void ref_tree_nodes(RefTree* r, int* ints, double* geom, int* nbr, int* sil, int
     }
 }
 
+#if !defined(REF_NCC)
 // complex_image_to_source at arbitrary points (nearest node per point).
 void ref_points(RefTree* r, const RefLens* L, long long n, const double* zx, const double* zy, double* wx, double* wy,
                 int nthreads) {
@@ -202,6 +206,8 @@ void ref_points(RefTree* r, const RefLens* L, long long n, const double* zx, con
     wy[i] = w.im;
   }
 }
+
+#endif
 
 #if defined(REF_IPM)
 // shoot_cells_kernel (ipm_functions.cuh:112-230) over the whole cell lattice,
@@ -329,6 +335,32 @@ void ref_ccf_run(RefTree* r, const RefLens* L, int nroots, int nphi, int nb, dou
                                   L->rect, corner, L->approx, L->taylor_smooth, mu_len);
   delete[] fin;
   delete[] errs;
+}
+#endif
+
+#if defined(REF_NCC)
+// The map of include/ncc.cuh (calculate_num_caustic_crossings, :235-327) with
+// the reference's own kernels on one host thread: the crossings on the
+// 2^os times finer map, then os rounds of the 2 x 2 maximum and the row /
+// column shifts. caus: nrows x ncols complex values; out: npy x npx.
+void ref_ncc_run(const double* caus, int nrows, int ncols, double cy1, double cy2, double hl1, double hl2, int npx,
+                 int npy, int os, int* out) {
+  serial_grid();
+  Complex<int> np(npx << os, npy << os);
+  int* num = new int[(size_t)np.re * np.im]();
+  unsigned long long percentage = 1;
+  Complex<T>* c = const_cast<Complex<T>*>(reinterpret_cast<const Complex<T>*>(caus));
+  find_num_caustic_crossings_kernel<T>(c, nrows, ncols, Complex<T>(cy1, cy2), Complex<T>(hl1, hl2), num, np,
+                                       &percentage, 0);
+  for (int i = 0; i < os; i++) {
+    np.re >>= 1;
+    np.im >>= 1;
+    reduce_pix_array_kernel<T>(num, np);
+    for (int j = 1; j < np.re; j++) shift_pix_column_kernel<T>(num, np, j);
+    for (int j = 1; j < np.im; j++) shift_pix_row_kernel<T>(num, np, j);
+  }
+  for (long long q = 0; q < (long long)npx * npy; q++) out[q] = num[q];
+  delete[] num;
 }
 #endif
 

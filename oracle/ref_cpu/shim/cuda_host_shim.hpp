@@ -63,6 +63,10 @@ inline cudaError_t cudaFree(void* p) {
   return cudaSuccess;
 }
 
+// integer min / max of the device math library
+inline int max(int a, int b) { return a > b ? a : b; }
+inline int min(int a, int b) { return a < b ? a : b; }
+
 // atomics (real atomics: emulated launches may run on several host threads)
 template <typename T, typename U>
 inline T atomicAdd(T* a, U v) {
