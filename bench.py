@@ -413,8 +413,32 @@ def ccf_measure():
                                  "caustics_ms": c.value("t_caustics") * 1e3, "points_per_s": pts / t,
                                  "max_error_inv_mu": c.value("max_error"),
                                  "expansion_order": int(c.value("expansion_order"))}
+            res[f"stars_{n}"]["ncc"] = ncc_measure(c.caustics)
             c.close()
     return res
+
+
+def ncc_hl(caus):
+    """Half length of a square NCC region holding the caustics' central part."""
+    return float(np.quantile(np.abs(caus[..., :2]).ravel(), 0.9))
+
+
+def ncc_measure(caus, npix=1000, over_sample=2):
+    """Caustic-crossing map (NCC, 1000^2 pixels, over_sample 2) of a CCF run's
+    caustics: device time of the crossings and the block maximum."""
+    import irs_b200
+    hl = ncc_hl(caus)
+    n = irs_b200.NCC(half_length_y1=hl, half_length_y2=hl, num_pixels_y1=npix, num_pixels_y2=npix,
+                     over_sample=over_sample, write_histograms=False)
+    n.set_caustics(caus)
+    n.run()
+    n.run()  # warm
+    t = n.value("t_ncc") + n.value("t_reduce")
+    out = {"half_length": hl, "segments": int(caus.shape[0] * (caus.shape[1] - 1)), "pixels": npix * npix,
+           "over_sample": over_sample, "ms": t * 1e3, "pixels_per_s": npix * npix / t,
+           "max_crossings": int(n.value("max_num"))}
+    n.close()
+    return out
 
 
 def ccf_cpu_reference(gpu_res, cases=(137, 400)):
@@ -437,7 +461,7 @@ def ccf_cpu_reference(gpu_res, cases=(137, 400)):
             init = ccf_ref.initial_roots(stars, 2 * n, 100, 1, rad)
             lens = po.lens(0.3, 0.3, float(np.sum(stars[:, 2]) / rad ** 2), 1.0, 0, 1, 1, (rad, 0.0))
             t0 = time.perf_counter()
-            rc, _, _, rme, _ = po.ref_ccf(stars, lens, rad * 1.1, init, 100, 1)
+            rc, rw, _, rme, _ = po.ref_ccf(stars, lens, rad * 1.1, init, 100, 1)
             t_cpu = time.perf_counter() - t0
             sf = os.path.join(td, f"s{n}.bin")
             ccf_write_stars(sf, stars, rad)
@@ -453,6 +477,23 @@ def ccf_cpu_reference(gpu_res, cases=(137, 400)):
             out[f"stars_{n}"] = {"seconds": t_cpu, "cores": 1, "max_error_inv_mu": rme,
                                  "gpu_seconds": t_gpu, "speedup": t_cpu / t_gpu,
                                  "max_curve_deviation": float(np.abs(rc - g[perm]).max())}
+            if n == cases[0]:  # the reference's NCC on these caustics (1000^2, over_sample 2)
+                caus = rw  # the reference's caustics
+                hl = ncc_hl(np.stack([caus.real, caus.imag], -1))
+                t0 = time.perf_counter()
+                ref_map = po.ref_ncc(caus, (0, 0), (hl, hl), (1000, 1000), 2)
+                t_ref = time.perf_counter() - t0
+                import irs_b200
+                nn = irs_b200.NCC(half_length_y1=hl, half_length_y2=hl, num_pixels_y1=1000, num_pixels_y2=1000,
+                                  over_sample=2, write_histograms=False)
+                nn.set_caustics(caus)
+                nn.run()
+                nn.run()
+                t_g = nn.value("t_ncc") + nn.value("t_reduce")
+                out["ncc_reference"] = {"seconds": t_ref, "cores": 1, "gpu_seconds": t_g, "speedup": t_ref / t_g,
+                                        "map_equal": bool(np.array_equal(nn.num_caustic_crossings, ref_map)),
+                                        "sample": f"caustics of the {n}-star CCF of the reference, 1000^2, x4"}
+                nn.close()
     return out
 
 
