@@ -17,6 +17,7 @@ import pytest
 from scipy.optimize import linear_sum_assignment
 
 from oracle import ccf_ref
+from oracle import pyoracle as po
 
 pytestmark = pytest.mark.gpu
 
@@ -122,4 +123,42 @@ def test_ccf_rejects_bad_input():
     c.lib.set_num_branches(c.obj, 3)  # num_phi is not a multiple of 2 * num_branches
     with pytest.raises(Exception, match="Error running CCF"):
         c.run()
+    c.close()
+
+
+@pytest.mark.skipif(not po.ref_ccf_available(),
+                    reason="reference CCF library not built (oracle/Makefile ref)")
+@pytest.mark.parametrize("approx", [1, 0])
+def test_ccf_rectangular_matches_reference(tmp_path, approx):
+    """Rectangular fields (the smooth sheet's derivatives of
+    alpha_smooth.cuh:141-300, and for approx the extra roots of its Taylor
+    series) against the reference's own CCF kernels run on the host: at every
+    phi the two sets of critical-curve points (and their caustics) agree.
+    Sets, not labels: the two update schemes may follow a curve through a
+    near-degenerate point on different roots."""
+    from irs_b200 import CCF
+    n = 24
+    rng = np.random.default_rng(21 + approx)
+    cx, cy = 8.0, 6.0  # kappa_star about 0.29
+    stars = np.stack([rng.uniform(-cx, cx, n), rng.uniform(-cy, cy, n), rng.uniform(0.5, 1.0, n)], 1)
+    sf = str(tmp_path / "rect.bin")
+    with open(sf, "wb") as f:
+        f.write(struct.pack("ii", n, 1))
+        f.write(struct.pack("ddd", cx, cy, 1.0))
+        f.write(np.ascontiguousarray(stars, np.float64).tobytes())
+    nphi = 20
+    c = CCF(kappa_tot=0.5, shear=0.2, starfile=sf, approx=bool(approx), num_phi=nphi, write_caustics=True)
+    c.run()
+    assert c.value("max_error") < 1e-8
+    ts = int(c.value("taylor_smooth"))
+    lens = po.lens(0.5, 0.2, c.kappa_star, 1.0, 1, approx, ts, (cx, cy))
+    init = ccf_ref.initial_roots(stars, c.num_roots, nphi, 1, np.hypot(cx, cy))
+    rc, rw, _, rme, _ = po.ref_ccf(stars, lens, max(cx, cy) * 1.1, init, nphi, 1)
+    assert 0 <= rme < 1e-8
+    g, gw = as_complex(c.critical_curves), as_complex(c.caustics)
+    for k in range(g.shape[1]):
+        d = np.abs(rc[:, k][:, None] - g[:, k][None, :])
+        i, j = linear_sum_assignment(d)
+        assert d[i, j].max() < 1e-6
+        assert np.abs(rw[i, k] - gw[j, k]).max() < 1e-6
     c.close()
