@@ -6,7 +6,8 @@ Produces, under irs_b200/lib/:
   lib_ccf.so                      critical curves, double (reference lib_ccf.so ABI)
   lib_ncc.so                      caustic-crossing maps, double (reference lib_ncc.so ABI)
 and under irs_b200/bin/ the command-line tools of the reference
-(src/main_ipm_irs.cu): ipm_gpu, ipm_gpu_double, irs_gpu, irs_gpu_double.
+(src/main_ipm_irs.cu, src/main_ccf.cu, src/main_ncc.cu): ipm_gpu,
+ipm_gpu_double, irs_gpu, irs_gpu_double, ccf_gpu, ncc_gpu.
 
 Usage: python -m irs_b200.build [--jobs N] [--force]
 """
@@ -83,13 +84,13 @@ def build_one(name: str, defs, force: bool = False, extra=None, source: str = "c
     return out
 
 
-def build_exe(name: str, defs, force: bool = False) -> str:
+def build_exe(name: str, defs, force: bool = False, source: str = "cli.cu") -> str:
     os.makedirs(BINDIR, exist_ok=True)
     out = os.path.join(BINDIR, name)
     if not force and not _stale(out):
         return out
     flags = [f for f in NVCC_FLAGS if f not in ("-shared",)]
-    cmd = [nvcc()] + flags + list(defs) + ["-I", CSRC, os.path.join(CSRC, "cli.cu"), "-o", out + ".tmp",
+    cmd = [nvcc()] + flags + list(defs) + ["-I", CSRC, os.path.join(CSRC, source), "-o", out + ".tmp",
                                             "-lcurand"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
@@ -106,6 +107,8 @@ def build(force: bool = False, jobs: int = 4, extra=None, executables: bool = Tr
         futs.append(ex.submit(build_one, "lib_ncc.so", [], force, extra, "ncc_capi.cu"))
         if executables:
             futs += [ex.submit(build_exe, n, d, force) for n, d in EXECUTABLES.items()]
+            futs.append(ex.submit(build_exe, "ccf_gpu", [], force, "cli_ccf.cu"))
+            futs.append(ex.submit(build_exe, "ncc_gpu", [], force, "cli_ncc.cu"))
         return [f.result() for f in cf.as_completed(futs)]
 
 

@@ -53,3 +53,34 @@ def test_irs_cli_counts(gpu, tmp_path):
     assert counts.sum() == int(info["num_rays_received"])
     hist = np.loadtxt(tmp_path / "irs_numrays_numpixels.txt", dtype=np.int64)
     assert hist[:, 1].sum() == 96 * 96
+
+
+@pytest.mark.parametrize("name,opt", [("ccf_gpu", "--num_phi"), ("ncc_gpu", "--over_sample")])
+def test_ccf_ncc_usage_and_syntax_errors(name, opt):
+    r = run(name, "-h")
+    assert r.returncode == 255 and opt in r.stdout and "--outfile_prefix" in r.stdout
+    r = run(name, "-v")
+    assert r.returncode == 255 and "Invalid input syntax" in r.stderr
+    r = run(name, "--nope", "1")
+    assert r.returncode == 255 and "Unknown option --nope" in r.stderr
+    r = run(name, "-v", "abc")
+    assert r.returncode == 255 and "Invalid verbose input" in r.stderr
+
+
+@pytest.mark.gpu
+def test_ccf_then_ncc_cli(gpu, tmp_path):
+    """ccf_gpu writes the critical curves and caustics; ncc_gpu maps the
+    caustic crossings from ccf_caustics.bin, as the reference's tools do."""
+    pre = str(tmp_path) + "/"
+    r = run("ccf_gpu", "-v", 0, "-k", 0.3, "-y", 0.3, "-s", 0.1, "-ns", 40, "-np", 50, "-rs", 5, "-o", pre)
+    assert r.returncode == 0, r.stderr
+    info = dict(l.split() for l in open(tmp_path / "ccf_parameter_info.txt"))
+    assert abs(float(info["kappa_star"]) - 0.27) < 1e-9 and info["num_roots"] == "80"
+    assert float(info["max_error_1/mu"]) < 1e-8
+    nr, nc = np.fromfile(tmp_path / "ccf_caustics.bin", dtype=np.int32, count=2)
+    assert (nr, nc) == (80, 51)
+    r = run("ncc_gpu", "-v", 0, "-ip", pre, "-hly1", 4, "-hly2", 4, "-npy1", 100, "-npy2", 100, "-os", 1, "-o", pre)
+    assert r.returncode == 0, r.stderr
+    m = np.fromfile(tmp_path / "ncc_ncc.bin", dtype=np.int32)
+    assert list(m[:2]) == [100, 100] and m[2:].min() >= 0 and m[2:].max() >= 1
+    assert os.path.exists(tmp_path / "ncc_ncc_numpixels.txt")
