@@ -145,6 +145,32 @@ __device__ __forceinline__ cplx<double> recip(cplx<double> d) {
   return mk(d.re * inv, -d.im * inv);
 }
 
+// sum over k = lane, lane + 32, ... < n, k != skip, of 1 / (z - p[k]): four
+// independent accumulators (four reciprocals in flight per lane), added in a
+// fixed order.
+__device__ __forceinline__ cplx<double> lane_recip_sum(const double2* __restrict__ p, int n, cplx<double> z,
+                                                       int skip, int lane) {
+  cplx<double> acc[4];
+#pragma unroll
+  for (int u = 0; u < 4; u++) acc[u] = mk(0.0, 0.0);
+  int i = lane;
+  for (; i + 96 < n; i += 128) {
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int k = i + 32 * u;
+      const double2 w = p[k];
+      const cplx<double> r = recip(mk(z.re - w.x, z.im - w.y));
+      if (k != skip) acc[u] = cadd(acc[u], r);
+    }
+  }
+  for (; i < n; i += 32) {
+    const double2 w = p[i];
+    const cplx<double> r = recip(mk(z.re - w.x, z.im - w.y));
+    if (i != skip) acc[0] = cadd(acc[0], r);
+  }
+  return cadd(cadd(acc[0], acc[1]), cadd(acc[2], acc[3]));
+}
+
 __device__ __forceinline__ cplx<double> warp_sum(cplx<double> v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -197,12 +223,14 @@ __device__ __forceinline__ CcfField ccf_field_warp(const CcfParams& P, const Lea
 // where both sides start from the branch centre). Positions are read from
 // `src` (rows of the root array, or the chain's scratch row) and written to
 // `dst`; fin[ch][a] marks final roots, which are copied. One warp per root:
-// the lanes split the sums over all stars and over the chain's other roots
-// (strided, so a warp reads 32 consecutive positions at a time; the star and
-// root arrays stay in L1) and reduce them in a fixed order.
+// the lanes split the sums over all stars (their positions `spos`, in tree
+// order) and over the chain's other roots (strided, so a warp reads 32
+// consecutive positions at a time; both arrays stay in L1) and reduce them in
+// a fixed order.
 template <typename T>
 __global__ void __launch_bounds__(kCcfThreads) ccf_iterate(CcfParams P, LeafPtrs lp, DescentPtrs<T> dp,
-                                                           const StarRec<T>* __restrict__ stars, int j, int sides,
+                                                           const StarRec<T>* __restrict__ stars,
+                                                           const double2* __restrict__ spos, int j, int sides,
                                                            int from_scratch, double2* __restrict__ roots,
                                                            double2* __restrict__ scratch,
                                                            unsigned char* __restrict__ fin) {
@@ -233,15 +261,8 @@ __global__ void __launch_bounds__(kCcfThreads) ccf_iterate(CcfParams P, LeafPtrs
     return;
   }
   const cplx<double> f1 = cconj(d.d2wdzb2);  // d f0 / dz
-  cplx<double> ps = mk(0.0, 0.0), rs = mk(0.0, 0.0);
-  for (int i = lane; i < P.nstars; i += 32) ps = cadd(ps, recip(mk(z.re - double(stars[i].x), z.im - double(stars[i].y))));
-  for (int i = lane; i < P.nroots; i += 32)
-    if (i != a) {
-      const double2 w = src[i];
-      rs = cadd(rs, recip(mk(z.re - w.x, z.im - w.y)));
-    }
-  ps = warp_sum(ps);
-  rs = warp_sum(rs);
+  cplx<double> ps = warp_sum(lane_recip_sum(spos, P.nstars, z, -1, lane));
+  cplx<double> rs = warp_sum(lane_recip_sum(src, P.nroots, z, a, lane));
   if (lane != 0) return;
   if (!P.rect && !P.approx) ps = cadd(ps, recip(z));
   ps = cscale(ps, 2.0);

@@ -8,6 +8,7 @@
 #include "stars.cuh"
 
 #include <chrono>
+#include <functional>
 #include <fstream>
 #include <iostream>
 
@@ -215,6 +216,11 @@ class CCF {
     stars_out.resize(n);
     IRSB_CKR(cudaMemcpyAsync(stars_out.data(), d_stars_.p, size_t(n) * sizeof(StarRec<T>), cudaMemcpyDeviceToHost,
                              s));
+    IRSB_CKR(cudaStreamSynchronize(s));
+    std::vector<double2> pos(n);  // star positions in tree order, for the sums over all stars
+    for (int i = 0; i < n; i++) pos[i] = make_double2(double(stars_out[i].x), double(stars_out[i].y));
+    if (!d_spos_.alloc_exact(n)) return false;
+    IRSB_CKR(cudaMemcpyAsync(d_spos_.p, pos.data(), n * sizeof(double2), cudaMemcpyHostToDevice, s));
 
     // ---- roots
     const CcfParams Q = params();
@@ -229,23 +235,51 @@ class CCF {
     const int rpb = kCcfThreads / 32;  // roots per CTA (a warp each)
     const dim3 g0(ceil_div(num_roots, rpb), num_branches), g1(ceil_div(num_roots, rpb), nch);
     const int it0 = num_iters_init + (num_iters_init & 1), it1 = num_iters_step + (num_iters_step & 1);
-    IRSB_CKR(cudaEventRecord(e0_, s));
-    for (int i = 0; i < it0; i++) {  // branch centres (include/ccf.cuh:906-977)
-      ccf_iterate<T><<<g0, kCcfThreads, 0, s>>>(Q, lp, dp, d_stars_.p, 0, 1, i & 1, d_roots_.p, d_scratch_.p,
-                                                d_fin_.p);
-    }
-    IRSB_LAUNCH_CK("ccf_iterate (centres)");
-    IRSB_CKR(cudaEventRecord(e1_, s));
+    // The root finding is ~1000 short launches: each part is captured as a
+    // CUDA graph and replayed, so the launches cost no host round trips.
     const int half = num_phi / (2 * num_branches);
     const int gp = std::max(1, std::min(ceil_div(nch * num_roots, 256), 148 * 8));
-    for (int j = 1; j <= half; j++) {  // steps away from the centres (include/ccf.cuh:979-1037)
-      ccf_prepare<<<gp, 256, 0, s>>>(Q, j, d_roots_.p, d_fin_.p);
-      for (int i = 0; i < it1; i++)
-        ccf_iterate<T><<<g1, kCcfThreads, 0, s>>>(Q, lp, dp, d_stars_.p, j, 2, i & 1, d_roots_.p, d_scratch_.p,
-                                                  d_fin_.p);
+    cudaGraphExec_t centres = nullptr, steps = nullptr;
+    auto capture = [&](cudaGraphExec_t& exec, const std::function<void()>& launches) -> bool {
+      cudaGraph_t g = nullptr;
+      IRSB_CKR(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      launches();
+      const cudaError_t le = cudaGetLastError();
+      const cudaError_t ce = cudaStreamEndCapture(s, &g);
+      if (le != cudaSuccess || ce != cudaSuccess) {
+        std::cerr << "Error. Capturing the root finding failed: " << cudaGetErrorString(le != cudaSuccess ? le : ce)
+                  << "\n";
+        if (g) cudaGraphDestroy(g);
+        return false;
+      }
+      const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
+      cudaGraphDestroy(g);
+      return IRSB_CK(ie);
+    };
+    const bool ok_graphs =
+        capture(centres,
+                [&] {
+                  for (int i = 0; i < it0; i++)  // branch centres (include/ccf.cuh:906-977)
+                    ccf_iterate<T><<<g0, kCcfThreads, 0, s>>>(Q, lp, dp, d_stars_.p, d_spos_.p, 0, 1, i & 1,
+                                                              d_roots_.p, d_scratch_.p, d_fin_.p);
+                }) &&
+        capture(steps, [&] {
+          for (int j = 1; j <= half; j++) {  // steps away from the centres (include/ccf.cuh:979-1037)
+            ccf_prepare<<<gp, 256, 0, s>>>(Q, j, d_roots_.p, d_fin_.p);
+            for (int i = 0; i < it1; i++)
+              ccf_iterate<T><<<g1, kCcfThreads, 0, s>>>(Q, lp, dp, d_stars_.p, d_spos_.p, j, 2, i & 1, d_roots_.p,
+                                                        d_scratch_.p, d_fin_.p);
+          }
+        });
+    bool ok_run = ok_graphs;
+    if (ok_run) {
+      ok_run = IRSB_CK(cudaEventRecord(e0_, s)) && IRSB_CK(cudaGraphLaunch(centres, s)) &&
+               IRSB_CK(cudaEventRecord(e1_, s)) && IRSB_CK(cudaGraphLaunch(steps, s)) &&
+               IRSB_CK(cudaEventRecord(e2_, s)) && IRSB_CK(cudaStreamSynchronize(s));
     }
-    IRSB_LAUNCH_CK("ccf_iterate (steps)");
-    IRSB_CKR(cudaEventRecord(e2_, s));
+    if (centres) cudaGraphExecDestroy(centres);
+    if (steps) cudaGraphExecDestroy(steps);
+    if (!ok_run) return false;
     // ---- error bound in 1/mu over every root (include/ccf.cuh:1044-1069)
     IRSB_CKR(cudaMemsetAsync(d_stat_.p, 0, 2 * sizeof(unsigned long long), s));
     const long long total = (long long)rows * num_roots;
@@ -378,7 +412,7 @@ class CCF {
   TreeDev<T> tree_;
   FmmDev fmm_;
   LeafSet leaves_;
-  DevVec<double2> d_roots_, d_scratch_, d_ccs_, d_caus_;
+  DevVec<double2> d_roots_, d_scratch_, d_ccs_, d_caus_, d_spos_;
   DevVec<double> d_mu_;
   DevVec<unsigned char> d_fin_;
   DevVec<unsigned long long> d_stat_;
