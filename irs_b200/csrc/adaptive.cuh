@@ -43,22 +43,54 @@ constexpr int kAdaFeatures = 8;
 __host__ __device__ __forceinline__ int ada_level_of(int cls) { return 1 << cls; }
 __host__ __device__ __forceinline__ long long llmin_(long long a, long long b) { return a < b ? a : b; }
 
+// A leaf's near stars and local coefficients (FP32 records), in global
+// memory or staged in shared memory.
+// With the constants of the lens equation at the leaf (those of shoot_f32:
+// linear terms, pixel scales, the leaf centre's source position), computed
+// once per view.
+struct LeafView {
+  const float4* near;
+  const float2* coef;
+  int nn;
+  double cx, cy;
+  float inv_hl;
+  double lin_x, lin_y, scx, scy, pcx, pcy;
+};
+
+__device__ __forceinline__ LeafView make_leaf_view(const ShootParams& sp, const float4* near, const float2* coef,
+                                                   int nn, double cx, double cy, double hl) {
+  LeafView L;
+  L.near = near;
+  L.coef = coef;
+  L.nn = nn;
+  L.cx = cx;
+  L.cy = cy;
+  L.inv_hl = float(1.0 / hl);
+  L.lin_x = 1.0 - sp.kappa + sp.kstar + sp.gamma;
+  L.lin_y = 1.0 - sp.kappa + sp.kstar - sp.gamma;
+  L.scx = sp.npx / (2.0 * sp.hly_re);
+  L.scy = sp.npy / (2.0 * sp.hly_im);
+  L.pcx = ((L.lin_x * cx - sp.cy_re) + sp.hly_re) * L.scx;
+  L.pcy = ((L.lin_y * cy - sp.cy_im) + sp.hly_im) * L.scy;
+  return L;
+}
+
+__device__ __forceinline__ LeafView leaf_view(const ShootParams& sp, const LeafPtrs& lp, int leaf) {
+  return make_leaf_view(sp, lp.near32 + (size_t)leaf * kMaxStarsDirect, lp.coef32 + (size_t)leaf * kMaxOrder,
+                        lp.nnear[leaf], lp.cx[leaf], lp.cy[leaf], lp.hl[leaf]);
+}
+
 // Source position (pixel units, row axis flipped) of the lattice point (x, y)
-// evaluated with leaf `leaf`: the arithmetic of shoot_f32 for one point, so a
+// evaluated with leaf L: the arithmetic of shoot_f32 for one point, so a
 // base lattice point gets the same position from either kernel.
 template <bool GENERIC_SMOOTH>
-__device__ __forceinline__ double2 eval_point_f32(const ShootParams& sp, const LeafPtrs& lp, int leaf, double x,
-                                                  double y) {
-  const double lcx = lp.cx[leaf], lcy = lp.cy[leaf];
-  const float inv_hl = float(1.0 / lp.hl[leaf]);
-  const double lin_x = 1.0 - sp.kappa + sp.kstar + sp.gamma;
-  const double lin_y = 1.0 - sp.kappa + sp.kstar - sp.gamma;
-  const double scx = sp.npx / (2.0 * sp.hly_re), scy = sp.npy / (2.0 * sp.hly_im);
-  const double pcx = ((lin_x * lcx - sp.cy_re) + sp.hly_re) * scx;
-  const double pcy = ((lin_y * lcy - sp.cy_im) + sp.hly_im) * scy;
+__device__ __forceinline__ double2 eval_point_f32(const ShootParams& sp, const LeafView& L, double x, double y) {
+  const double lcx = L.cx, lcy = L.cy;
+  const float inv_hl = L.inv_hl;
+  const double lin_x = L.lin_x, lin_y = L.lin_y, scx = L.scx, scy = L.scy, pcx = L.pcx, pcy = L.pcy;
   const float ux = float(x - lcx), uy = float(y - lcy);
-  const int nn = lp.nnear[leaf];
-  const float4* near = lp.near32 + (size_t)leaf * kMaxStarsDirect;
+  const int nn = L.nn;
+  const float4* near = L.near;
   float sx = 0.f, sy = 0.f, cxr = 0.f, cyr = 0.f;
   for (int s0 = 0; s0 < nn; s0 += 4) {
     float bx = 0.f, by = 0.f;
@@ -78,7 +110,7 @@ __device__ __forceinline__ double2 eval_point_f32(const ShootParams& sp, const L
     cyr += (sy - (t - bb)) + (by - bb);
     sy = t;
   }
-  const float2* coef = lp.coef32 + (size_t)leaf * kMaxOrder;
+  const float2* coef = L.coef;
   const float dzr = ux * inv_hl, dzi = uy * inv_hl;
   float Ar = 0.f, Ai = 0.f;
   for (int k = sp.p - 1; k >= 0; k--) {
@@ -119,79 +151,116 @@ struct AdaGeom {
 
 // Corner (a, b) of tile t at level s, in the tile's corner grid
 // [0, ncell_x * s] x [0, ncell_y * s].
+// `stage`: the records of the tile's own leaf in shared memory, when the tile
+// has one (the values are those of the leaf in global memory).
 template <typename T, bool GENERIC_SMOOTH>
 __device__ __forceinline__ double2 tile_corner(const AdaGeom& g, const ShootParams& sp, const LeafPtrs& lp,
                                                const DescentPtrs<T>& dp, const double2* __restrict__ base_verts,
-                                               int tx, int ty, int s, int a, int b) {
+                                               int tx, int ty, int s, int a, int b,
+                                               const LeafView* stage = nullptr) {
   const long long i0 = (long long)tx * kAdaTile, j0 = (long long)ty * kAdaTile;
-  if (a % s == 0 && b % s == 0) {
-    const long long i = i0 + a / s, j = j0 + b / s;
+  const int sh = __ffs(s) - 1;  // levels are powers of two
+  if (((a | b) & (s - 1)) == 0) {
+    const long long i = i0 + (a >> sh), j = j0 + (b >> sh);
     return base_verts[j * (g.ncx + 1) + i];
   }
-  const long long F = (i0 * kAdaMaxLevel) + (long long)a * (kAdaMaxLevel / s);
-  const long long G = (j0 * kAdaMaxLevel) + (long long)b * (kAdaMaxLevel / s);
+  const long long F = (i0 * kAdaMaxLevel) + (long long)a * (kAdaMaxLevel >> sh);
+  const long long G = (j0 * kAdaMaxLevel) + (long long)b * (kAdaMaxLevel >> sh);
   const double x = fine_coord(g.base_x, g.rhs_x, F), y = fine_coord(g.base_y, g.rhs_y, G);
   const int own = dp.tile_leaf ? dp.tile_leaf[ty * g.ntx + tx] : -1;  // the descent's answer, when uniform
-  return eval_point_f32<GENERIC_SMOOTH>(sp, lp, own >= 0 ? own : descend_leaf(dp, x, y), x, y);
+  if (own >= 0 && stage) return eval_point_f32<GENERIC_SMOOTH>(sp, *stage, x, y);
+  return eval_point_f32<GENERIC_SMOOTH>(sp, leaf_view(sp, lp, own >= 0 ? own : descend_leaf(dp, x, y)), x, y);
+}
+
+// Corner (a, b) of refined tile t (level s, corner grid wa x hb): points on an
+// edge shared with a coarser neighbour (tile_level, per tile) are placed on
+// that neighbour's edge segment; without tile_level every point is evaluated.
+template <typename T, bool GENERIC_SMOOTH>
+__device__ __forceinline__ double2 refine_point(const AdaGeom& g, const ShootParams& sp, const LeafPtrs& lp,
+                                                const DescentPtrs<T>& dp, const double2* __restrict__ base_verts,
+                                                const int* __restrict__ tile_level, int t, int tx, int ty, int s,
+                                                int a, int b, int wa, int hb, const LeafView* stage) {
+  // neighbour across the edge this point lies on (a point on two edges is a
+  // tile corner, hence a base point)
+  int nlev = s;
+  bool along_b = false;  // the edge runs along b (left / right edge)
+  if (!tile_level) {
+    // isolated tiles (labels, audit): every point evaluated
+  } else if (a == 0 && tx > 0) {
+    nlev = tile_level[t - 1];
+    along_b = true;
+  } else if (a == wa && tx + 1 < g.ntx && wa == kAdaTile * s) {
+    nlev = tile_level[t + 1];
+    along_b = true;
+  } else if (b == 0 && ty > 0) {
+    nlev = tile_level[t - g.ntx];
+  } else if (b == hb && ty + 1 < g.nty && hb == kAdaTile * s) {
+    nlev = tile_level[t + g.ntx];
+  }
+  if (nlev < s && ((a | b) & (s - 1)) != 0) {  // levels are powers of two
+    const int step = s >> (__ffs(nlev) - 1);
+    const int u = along_b ? b : a;
+    const int u0 = u & ~(step - 1), u1 = u0 + step;
+    const double2 p0 = along_b ? tile_corner<T, GENERIC_SMOOTH>(g, sp, lp, dp, base_verts, tx, ty, s, a, u0, stage)
+                               : tile_corner<T, GENERIC_SMOOTH>(g, sp, lp, dp, base_verts, tx, ty, s, u0, b, stage);
+    const double2 p1 = along_b ? tile_corner<T, GENERIC_SMOOTH>(g, sp, lp, dp, base_verts, tx, ty, s, a, u1, stage)
+                               : tile_corner<T, GENERIC_SMOOTH>(g, sp, lp, dp, base_verts, tx, ty, s, u1, b, stage);
+    const double f = double(u - u0) / double(step);
+    return make_double2(p0.x + (p1.x - p0.x) * f, p0.y + (p1.y - p0.y) * f);
+  }
+  return tile_corner<T, GENERIC_SMOOTH>(g, sp, lp, dp, base_verts, tx, ty, s, a, b, stage);
 }
 
 // Refined corner grids of the tiles in `list` (all at level s), written at
-// out + slot * stride with row stride ncell_x * s + 1. One thread per corner.
-// Points on an edge shared with a coarser neighbour (tile_level, per tile) are
-// placed on that neighbour's edge segment; without tile_level every point is
-// evaluated.
+// out + slot * stride with row stride ncell_x * s + 1; one CTA per band of
+// kAdaBandRows corner rows of a tile (refine_point for each corner). When
+// every point of the tile belongs to one leaf (DescentPtrs::tile_leaf), its
+// near stars and local coefficients are staged in shared memory and the
+// band's corners read them as broadcasts; the other tiles take the descent
+// per point.
+constexpr int kAdaBandRows = 16;
+__host__ __device__ __forceinline__ long long ada_band_items(long long ntiles, int s) {
+  return ntiles * ((kAdaTile * s + 1 + kAdaBandRows - 1) / kAdaBandRows);
+}
 template <typename T, bool GENERIC_SMOOTH>
-__global__ void __launch_bounds__(256) ada_refine_corners(AdaGeom g, ShootParams sp, LeafPtrs lp, DescentPtrs<T> dp,
-                                                          const double2* __restrict__ base_verts,
-                                                          const int* __restrict__ tile_level,
-                                                          const int* __restrict__ list, int nlist, int s,
-                                                          long long stride, double2* __restrict__ out) {
-  const int side = kAdaTile * s + 1;
-  const long long per_tile = (long long)side * side;
-  const long long total = per_tile * nlist;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-       q += (long long)gridDim.x * blockDim.x) {
-    const int slot = int(q / per_tile);
-    const int rem = int(q - (long long)slot * per_tile);
-    int b = rem / side, a = rem - b * side;
+__global__ void __launch_bounds__(256) ada_refine_tiles(AdaGeom g, ShootParams sp, LeafPtrs lp, DescentPtrs<T> dp,
+                                                        const double2* __restrict__ base_verts,
+                                                        const int* __restrict__ tile_level,
+                                                        const int* __restrict__ list, int nlist, int s,
+                                                        long long stride, double2* __restrict__ out) {
+  __shared__ float4 s_near[kMaxStarsDirect];
+  __shared__ float2 s_coef[kMaxOrder];
+  __shared__ LeafView s_view;
+  const int nbands = (kAdaTile * s + 1 + kAdaBandRows - 1) / kAdaBandRows;
+  for (long long item = blockIdx.x; item < (long long)nlist * nbands; item += gridDim.x) {
+    const int slot = int(item / nbands), band = int(item - (long long)slot * nbands);
     const int t = list[slot];
+    const int leaf = dp.tile_leaf ? dp.tile_leaf[t] : -1;  // CTA-uniform
+    if (leaf >= 0) {
+      if (threadIdx.x < kMaxStarsDirect) s_near[threadIdx.x] = lp.near32[(size_t)leaf * kMaxStarsDirect + threadIdx.x];
+      if (threadIdx.x >= 64 && threadIdx.x < 64 + kMaxOrder)
+        s_coef[threadIdx.x - 64] = lp.coef32[(size_t)leaf * kMaxOrder + threadIdx.x - 64];
+      if (threadIdx.x == 0) s_view = make_leaf_view(sp, s_near, s_coef, lp.nnear[leaf], lp.cx[leaf], lp.cy[leaf], lp.hl[leaf]);
+    }
+    __syncthreads();
+    const LeafView* stage = leaf >= 0 ? &s_view : nullptr;
     const int tx = t % g.ntx, ty = t / g.ntx;
-    const int ncx_t = int(llmin_(kAdaTile, g.ncx - (long long)tx * kAdaTile));
-    const int ncy_t = int(llmin_(kAdaTile, g.ncy - (long long)ty * kAdaTile));
-    const int wa = ncx_t * s, hb = ncy_t * s;  // corner grid extent of this (possibly partial) tile
-    if (a > wa || b > hb) continue;
-    // neighbour across the edge this point lies on (a point on two edges is a
-    // tile corner, hence a base point)
-    int nlev = s;
-    bool along_b = false;  // the edge runs along b (left / right edge)
-    if (!tile_level) {
-      // isolated tiles (labels, audit): every point evaluated
-    } else if (a == 0 && tx > 0) {
-      nlev = tile_level[t - 1];
-      along_b = true;
-    } else if (a == wa && tx + 1 < g.ntx && wa == kAdaTile * s) {
-      nlev = tile_level[t + 1];
-      along_b = true;
-    } else if (b == 0 && ty > 0) {
-      nlev = tile_level[t - g.ntx];
-    } else if (b == hb && ty + 1 < g.nty && hb == kAdaTile * s) {
-      nlev = tile_level[t + g.ntx];
+    const int wa = int(llmin_(kAdaTile, g.ncx - (long long)tx * kAdaTile)) * s;
+    const int hb = int(llmin_(kAdaTile, g.ncy - (long long)ty * kAdaTile)) * s;
+    const int w1 = wa + 1, b0 = band * kAdaBandRows, b1 = min(hb + 1, b0 + kAdaBandRows);
+    double2* o = out + (long long)slot * stride;
+    // corners (a, b) of the band in row-major order, thread k taking k, k + 256, ...
+    int b = b0 + int(threadIdx.x) / w1, a = int(threadIdx.x) - (b - b0) * w1;
+    while (b < b1) {
+      o[(long long)b * w1 + a] =
+          refine_point<T, GENERIC_SMOOTH>(g, sp, lp, dp, base_verts, tile_level, t, tx, ty, s, a, b, wa, hb, stage);
+      a += blockDim.x;
+      while (a >= w1) {
+        a -= w1;
+        b++;
+      }
     }
-    double2 p;
-    if (nlev < s && !(a % s == 0 && b % s == 0)) {
-      const int step = s / nlev;
-      const int u = along_b ? b : a;
-      const int u0 = (u / step) * step, u1 = u0 + step;
-      const double2 p0 = along_b ? tile_corner<T, GENERIC_SMOOTH>(g, sp, lp, dp, base_verts, tx, ty, s, a, u0)
-                                 : tile_corner<T, GENERIC_SMOOTH>(g, sp, lp, dp, base_verts, tx, ty, s, u0, b);
-      const double2 p1 = along_b ? tile_corner<T, GENERIC_SMOOTH>(g, sp, lp, dp, base_verts, tx, ty, s, a, u1)
-                                 : tile_corner<T, GENERIC_SMOOTH>(g, sp, lp, dp, base_verts, tx, ty, s, u1, b);
-      const double f = double(u - u0) / double(step);
-      p = make_double2(p0.x + (p1.x - p0.x) * f, p0.y + (p1.y - p0.y) * f);
-    } else {
-      p = tile_corner<T, GENERIC_SMOOTH>(g, sp, lp, dp, base_verts, tx, ty, s, a, b);
-    }
-    out[(long long)slot * stride + (long long)b * (wa + 1) + a] = p;
+    __syncthreads();  // the stage is rewritten for the next tile
   }
 }
 

@@ -42,7 +42,7 @@ class AdaptiveIPM {
   long long refine_cap = 0;      // corner positions in the refinement buffer (0: automatic)
   // chunks of at least this many tiles of one level are refined by the tiled
   // lens kernel over the level-s lattice (refine_tiled), smaller ones point by
-  // point (ada_refine_corners)
+  // point (ada_refine_tiles)
   int tiled_min = 1 << 30;
   std::vector<float> net_w, net_mu, net_sig;  // FP32 master weights, feature standardisation
   float net_quantile = 0.8f;  // a tile takes the smallest level whose cumulative probability reaches this
@@ -259,14 +259,13 @@ class AdaptiveIPM {
     std::vector<DepositPiece<float>> pieces;
     for (size_t k0 = 0; k0 < tiles.size(); k0 += chunk) {
       const int n = int(std::min<size_t>(chunk, tiles.size() - k0));
-      const long long total = per * n;
-      const int grid = int(std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 32)));
+      const int grid = int(std::max<long long>(1, std::min<long long>(ada_band_items(n, kAdaMaxLevel), 148LL * 8)));
       if (generic_)
-        ada_refine_corners<T, true><<<grid, 256, 0, s>>>(g_, sp_, base.leaf_ptrs(), descent(), base.d_verts_.p,
-                                                         nullptr, d_list_.p + k0, n, kAdaMaxLevel, per, d_ref_.p);
+        ada_refine_tiles<T, true><<<grid, 256, 0, s>>>(g_, sp_, base.leaf_ptrs(), descent(), base.d_verts_.p,
+                                                       nullptr, d_list_.p + k0, n, kAdaMaxLevel, per, d_ref_.p);
       else
-        ada_refine_corners<T, false><<<grid, 256, 0, s>>>(g_, sp_, base.leaf_ptrs(), descent(), base.d_verts_.p,
-                                                          nullptr, d_list_.p + k0, n, kAdaMaxLevel, per, d_ref_.p);
+        ada_refine_tiles<T, false><<<grid, 256, 0, s>>>(g_, sp_, base.leaf_ptrs(), descent(), base.d_verts_.p,
+                                                        nullptr, d_list_.p + k0, n, kAdaMaxLevel, per, d_ref_.p);
       ada_tile_windows<<<std::min(n, 148 * 8), 256, 0, s>>>(g_, d_list_.p + k0, n, per, d_ref_.p, d_win_.p);
       IRSB_LAUNCH_CK("ada windows");
       IRSB_CKR(cudaMemcpyAsync(win.data(), d_win_.p, n * sizeof(int4), cudaMemcpyDeviceToHost, s));
@@ -491,17 +490,16 @@ class AdaptiveIPM {
         verts = d_ref_.p;
       } else if (L.s > 1) {
         const long long per = (long long)(kAdaTile * L.s + 1) * (kAdaTile * L.s + 1);
-        const long long total = per * L.nlist;
-        const int grid = int(std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 32)));
+        const int grid = int(std::max<long long>(1, std::min<long long>(ada_band_items(L.nlist, L.s), 148LL * 8)));
         if (generic_)
-          ada_refine_corners<T, true><<<grid, 256, 0, s>>>(g_, sp_, base.leaf_ptrs(), descent(), base.d_verts_.p,
-                                                           d_level_.p, d_list_.p + L.list_off, L.nlist, L.s, per,
-                                                           d_ref_.p);
+          ada_refine_tiles<T, true><<<grid, 256, 0, s>>>(g_, sp_, base.leaf_ptrs(), descent(), base.d_verts_.p,
+                                                         d_level_.p, d_list_.p + L.list_off, L.nlist, L.s, per,
+                                                         d_ref_.p);
         else
-          ada_refine_corners<T, false><<<grid, 256, 0, s>>>(g_, sp_, base.leaf_ptrs(), descent(), base.d_verts_.p,
-                                                            d_level_.p, d_list_.p + L.list_off, L.nlist, L.s, per,
-                                                            d_ref_.p);
-        IRSB_LAUNCH_CK("ada_refine_corners");
+          ada_refine_tiles<T, false><<<grid, 256, 0, s>>>(g_, sp_, base.leaf_ptrs(), descent(), base.d_verts_.p,
+                                                          d_level_.p, d_list_.p + L.list_off, L.nlist, L.s, per,
+                                                          d_ref_.p);
+        IRSB_LAUNCH_CK("ada_refine_tiles");
         verts = d_ref_.p;
       }
       const int grid = int(std::max<long long>(1, std::min<long long>(ceil_div(L.nchunks, 8), 148LL * 32)));
