@@ -197,7 +197,7 @@ def reference_arm(args):
     L = oracle_lens(m)
     factor = 2 * rx * ry * m.num_pixels_y1 * m.num_pixels_y2 / (4 * m.half_length_y1 * m.half_length_y2)
     use_ref = po.ref_available()
-    band_rows = 24
+    band_rows = 2048
 
     def step(k):
         """Seconds the full map takes: the tree and expansions once, plus a band
