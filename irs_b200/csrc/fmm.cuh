@@ -116,7 +116,16 @@ __global__ void fmm_m2m(int beg, int end, LevelRange lr, int p, const T* __restr
 
 // Local coefficients of the nodes of one level (>= 2): L2L from the parent,
 // then M2L over the same-level interaction list, then P2L over the
-// different-level list, accumulated in that order.
+// different-level list.
+//
+// One warp per node, split into G = 32 / (p + 1) groups of p + 1 lanes (lane
+// l of a group computes order l). The per-interaction quantities every order
+// needs (the source's reciprocal distance and the logarithms of the order-0
+// term) are computed once, interaction j (or star j) on lane j, and read by
+// the groups through shuffles; group g takes interactions g, g + G, ... and
+// the groups' sums are added into group 0 in group order (deterministic).
+// Each interaction term is evaluated with the reference's Horner ordering.
+static_assert(kMaxSameLevelIL <= 32, "one lane per same-level interaction");
 template <typename T>
 __global__ void fmm_local(int beg, int end, LevelRange lr, int p, const T* __restrict__ cx, const T* __restrict__ cy,
                           const T* __restrict__ hl, const int* __restrict__ parent, const int* __restrict__ sbeg,
@@ -125,73 +134,110 @@ __global__ void fmm_local(int beg, int end, LevelRange lr, int p, const T* __res
                           const StarRec<T>* __restrict__ stars, const double* __restrict__ btab,
                           const double2* __restrict__ mult, double2* loc) {
   lr.get(beg, end);
-  int lane = threadIdx.x & 31;
-  int warps = (gridDim.x * blockDim.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int P1 = p + 1;
+  const int G = 32 / P1;
+  const int g = lane / P1, l = lane - g * P1;
+  const bool grp = g < G;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  const cplx<double> zero = mk(0.0, 0.0);
   for (int k = beg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < end; k += warps) {
-    if (lane > p) continue;
     const double ccx = cx[k], ccy = cy[k], h = hl[k];
-    // L2L
-    int pa = parent[k];
-    const double2* cp = loc + (size_t)pa * (p + 1);
-    double hp = hl[pa];
-    cplx<double> dz = mk((ccx - double(cx[pa])) / hp, (ccy - double(cy[pa])) / hp);
-    cplx<double> r = mk(0.0, 0.0);
-    for (int i = p; i >= 1; i--) {
-      r = cadd(r, cscale(ld2(cp + i), binom(btab, i, lane)));
-      r = cmul(r, dz);
+    cplx<double> acc = zero;
+    // L2L (group 0)
+    if (g == 0) {
+      const int pa = parent[k];
+      const double2* cp = loc + (size_t)pa * P1;
+      const double hp = hl[pa];
+      const cplx<double> dz = mk((ccx - double(cx[pa])) / hp, (ccy - double(cy[pa])) / hp);
+      cplx<double> r = zero;
+      for (int i = p; i >= 1; i--) {
+        r = cadd(r, cscale(ld2(cp + i), binom(btab, i, l)));
+        r = cmul(r, dz);
+      }
+      r = cdiv(r, cpowi(dz, l));
+      acc = cdivr(r, double(1u << l));
     }
-    r = cdiv(r, cpowi(dz, lane));
-    r = cdivr(r, double(1u << lane));
-    cplx<double> acc = r;
-    // M2L
-    int ns = n_sil[k];
-    for (int j = 0; j < ns; j++) {
-      int f = sil[k * kMaxSameLevelIL + j];
-      const double2* b = mult + (size_t)f * (p + 1);
-      double hf = hl[f];
-      cplx<double> d = mk((double(cx[f]) - ccx) / hf, (double(cy[f]) - ccy) / hf);
-      cplx<double> md = cneg(d);
-      const cplx<double> imd = cdiv(mk(1.0, 0.0), md);
-      cplx<double> t = mk(0.0, 0.0);
-      if (lane == 0) {
-        for (int i = p; i >= 1; i--) {
-          t = cadd(t, ld2(b + i));
-          t = cmul(t, imd);
-        }
-        cplx<double> b0 = ld2(b);
-        t = cadd(t, cmul(b0, clog_(md)));
-        t = cadd(t, cscale(b0, log(hf)));
+    // M2L: interaction j's source, 1 / (-dz), log(-dz) and log(hl_from) on lane j
+    const int ns = n_sil[k];
+    int fj = 0;
+    cplx<double> imdj = zero, lgj = zero;
+    double lhj = 0.0;
+    if (lane < ns) {
+      fj = sil[k * kMaxSameLevelIL + lane];
+      const double hf = hl[fj];
+      const cplx<double> md = cneg(mk((double(cx[fj]) - ccx) / hf, (double(cy[fj]) - ccy) / hf));
+      imdj = cdiv(mk(1.0, 0.0), md);
+      lgj = clog_(md);
+      lhj = log(hf);
+    }
+    for (int j0 = 0; j0 < ns; j0 += G) {
+      const int j = j0 + g;
+      const int src = j < 32 ? j : 31;
+      const int f = __shfl_sync(0xffffffffu, fj, src);
+      const cplx<double> imd = mk(__shfl_sync(0xffffffffu, imdj.re, src), __shfl_sync(0xffffffffu, imdj.im, src));
+      const cplx<double> lg = mk(__shfl_sync(0xffffffffu, lgj.re, src), __shfl_sync(0xffffffffu, lgj.im, src));
+      const double lh = __shfl_sync(0xffffffffu, lhj, src);
+      if (!grp || j >= ns) continue;
+      const double2* b = mult + (size_t)f * P1;
+      cplx<double> t = zero;
+      for (int i = p; i >= 1; i--) {  // C(l + i - 1, i - 1) is 1 for l = 0
+        t = cadd(t, cscale(ld2(b + i), binom(btab, l + i - 1, i - 1)));
+        t = cmul(t, imd);
+      }
+      const cplx<double> b0 = ld2(b);
+      if (l == 0) {
+        t = cadd(t, cmul(b0, lg));
+        t = cadd(t, cscale(b0, lh));
       } else {
-        for (int i = p; i >= 1; i--) {
-          t = cadd(t, cscale(ld2(b + i), binom(btab, lane + i - 1, i - 1)));
-          t = cmul(t, imd);
-        }
-        t = csub(t, cdivr(ld2(b), double(lane)));
-        t = cmul(t, cpowi(cneg(imd), lane));  // 1 / d^l
+        t = csub(t, cdivr(b0, double(l)));
+        t = cmul(t, cpowi(cneg(imd), l));  // 1 / dz^l
       }
       acc = cadd(acc, t);
     }
-    // P2L
-    int nd = n_dil[k];
-    for (int j = 0; j < nd; j++) {
-      int f = dil[k * kMaxDiffLevelIL + j];
-      int sb = sbeg[f], sn = scnt[f];
-      cplx<double> t = mk(0.0, 0.0);
-      for (int i = 0; i < sn; i++) {
-        StarRec<T> s = stars[sb + i];
-        cplx<double> d = mk((double(s.x) - ccx) / h, (double(s.y) - ccy) / h);
-        double m = double(s.m);
-        if (lane == 0) {
-          t = cadd(t, cscale(clog_(cneg(d)), m));
-          t.re += m * log(h);
-        } else {
-          // m / (l d^l) = (m / l) (1/d)^l
-          t = csub(t, cscale(cpowi(cdiv(mk(1.0, 0.0), d), lane), m / double(lane)));
+    // P2L: star u of each list's chunk of 32: 1 / dz and log(-dz) on lane u
+    const int nd = n_dil[k];
+    const double lhk = nd > 0 ? log(h) : 0.0;
+    for (int q = 0; q < nd; q++) {
+      const int f = dil[k * kMaxDiffLevelIL + q];
+      const int sb = sbeg[f], sn = scnt[f];
+      cplx<double> t = zero;
+      for (int i0 = 0; i0 < sn; i0 += 32) {
+        cplx<double> idu = zero, lgu = zero;
+        double mu = 0.0;
+        if (i0 + lane < sn) {
+          const StarRec<T> st = stars[sb + i0 + lane];
+          const cplx<double> d = mk((double(st.x) - ccx) / h, (double(st.y) - ccy) / h);
+          mu = double(st.m);
+          idu = cdiv(mk(1.0, 0.0), d);
+          lgu = clog_(cneg(d));
+        }
+        const int cnt = min(32, sn - i0);
+        for (int u0 = 0; u0 < cnt; u0 += G) {
+          const int u = u0 + g;
+          const int src = u < 32 ? u : 31;
+          const cplx<double> id = mk(__shfl_sync(0xffffffffu, idu.re, src), __shfl_sync(0xffffffffu, idu.im, src));
+          const cplx<double> lg = mk(__shfl_sync(0xffffffffu, lgu.re, src), __shfl_sync(0xffffffffu, lgu.im, src));
+          const double m = __shfl_sync(0xffffffffu, mu, src);
+          if (!grp || u >= cnt) continue;
+          if (l == 0) {
+            t = cadd(t, cscale(lg, m));
+            t.re += m * lhk;
+          } else {
+            // m / (l d^l) = (m / l) (1/d)^l
+            t = csub(t, cscale(cpowi(id, l), m / double(l)));
+          }
         }
       }
       acc = cadd(acc, t);
     }
-    st2(&loc[(size_t)k * (p + 1) + lane], acc);
+    // the groups' sums into group 0, in group order
+    for (int gg = 1; gg < G; gg++) {
+      const int src = min(l + gg * P1, 31);
+      const cplx<double> o = mk(__shfl_sync(0xffffffffu, acc.re, src), __shfl_sync(0xffffffffu, acc.im, src));
+      if (g == 0) acc = cadd(acc, o);
+    }
+    if (g == 0) st2(&loc[(size_t)k * P1 + l], acc);
   }
 }
 
