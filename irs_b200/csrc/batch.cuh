@@ -94,26 +94,6 @@ __global__ void batch_tree_roots(int R, const T* __restrict__ root_hl, const lon
   }
 }
 
-// After the split scan of level l: the next level's extent, or a stop with an
-// error when the node capacity or the level limit would be exceeded.
-__global__ void batch_tree_advance(int l, int nlev, int* off, int* lvl_n, const long long* __restrict__ nsplit_p,
-                                   int node_cap, int* stop, int* dstat) {
-  const int end = off[l + 1];
-  long long nsplit = *stop ? 0 : *nsplit_p;
-  if (nsplit > 0 && l == nlev - 1) {
-    atomicOr(&dstat[1], kErrLevelOverflow);
-    *stop = 1;
-    nsplit = 0;
-  }
-  if (end + 4 * nsplit > node_cap) {
-    atomicOr(&dstat[1], kErrNodeOverflow);
-    *stop = 1;
-    nsplit = 0;
-  }
-  off[l + 2] = end + int(4 * nsplit);
-  lvl_n[l + 1] = int(4 * nsplit);
-}
-
 __global__ void batch_levels(const int* __restrict__ off, int nlev, const int* __restrict__ level,
                              const int* __restrict__ rid, int* levels_r) {
   const int n = off[nlev];
@@ -582,13 +562,18 @@ class BatchMaker {
       const LevelRange lr{d_off_.p, l};
       tree_near_count<<<G, 256, 0, s>>>(0, 0, lr, t.scnt.p, t.nbr.p, t.n_nbr.p, t.split.p, dstat);
       if (!exclusive_scan_dev<int>(t.split.p, d_lvl_n_.p + l, node_cap_, t.rank.p, t.scan, s)) return false;
-      batch_tree_advance<<<1, 1, 0, s>>>(l, nlev, d_off_.p, d_lvl_n_.p, t.scan.sum.p, ncap, d_stop_.p, dstat);
+      tree_advance_level<<<1, 1, 0, s>>>(l, nlev, d_off_.p, d_lvl_n_.p, t.scan.sum.p, ncap, d_stop_.p, dstat);
       tree_make_children<T><<<G, 256, 0, s>>>(0, 0, 0, lr, d_stop_.p, t.split.p, t.rank.p, t.cx.p, t.cy.p, t.hl.p,
                                               t.level.p, t.parent.p, t.child0.p, t.sbeg.p, t.scnt.p, t.rid.p,
                                               t.n_nbr.p, t.n_sil.p, t.n_dil.p, t.lox.p, t.hix.p, t.loy.p, t.hiy.p);
       if (l + 1 < nlev) {
-        tree_partition_stars<T><<<G, 256, 0, s>>>(0, 0, lr, d_stop_.p, t.split.p, t.cx.p, t.cy.p, t.child0.p,
-                                                  t.sbeg.p, t.scnt.p, d_stars_.p, t.tmp_stars.p);
+        if (l < 2)  // a few nodes per realization, many stars each
+          tree_partition_stars<T, 1024><<<G, 1024, 0, s>>>(0, 0, lr, d_stop_.p, t.split.p, t.cx.p, t.cy.p,
+                                                            t.child0.p, t.sbeg.p, t.scnt.p, d_stars_.p,
+                                                            t.tmp_stars.p);
+        else
+          tree_partition_stars<T><<<G, 256, 0, s>>>(0, 0, lr, d_stop_.p, t.split.p, t.cx.p, t.cy.p, t.child0.p,
+                                                    t.sbeg.p, t.scnt.p, d_stars_.p, t.tmp_stars.p);
         tree_set_neighbors<T><<<G, 256, 0, s>>>(0, 0, LevelRange{d_off_.p, l + 1}, t.cx.p, t.cy.p, t.hl.p,
                                                 t.parent.p, t.child0.p, t.scnt.p, t.nbr.p, t.n_nbr.p, t.sil.p,
                                                 t.n_sil.p, t.dil.p, t.n_dil.p, dstat);

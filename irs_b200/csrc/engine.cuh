@@ -229,7 +229,7 @@ class MapMaker {
     const int n = prm.num_stars;
     IRSB_CKR(cudaEventRecord(ev0_, stream_));
     if (!build_tree<T>(tree_, d_stars_.p, n, prm.root_half_length, stream_)) return false;
-    launches += 1 + 5LL * tree_.levels + 2;
+    launches += tree_.launches;
     prm.tree_levels = tree_.levels;
     prm.expansion_order =
         prm.expansion_order_override > 0 ? prm.expansion_order_override : expansion_order_of(prm);

@@ -27,6 +27,8 @@
 #include "devutil.cuh"
 #include "params.hpp"
 
+#include <algorithm>
+#include <cstdio>
 #include <vector>
 
 namespace irsb {
@@ -63,7 +65,9 @@ struct TreeDev {
   DevVec<long long> rank;
   DevVec<int> dstat;  // [0] max near count, [1] error bits
   ScanScratch scan;
-  DevVec<StarRec<T>> tmp_stars;
+  DevVec<StarRec<T>> tmp_stars, star_backup;
+  DevVec<int> d_off, d_lvl_n, d_stop;  // level offsets and sizes on the device
+  long long launches = 0;              // kernels the last build launched
 };
 
 template <typename T>
@@ -191,11 +195,12 @@ __device__ __forceinline__ int star_quadrant(T x, T y, T cx, T cy) {
   return 3;
 }
 
-// Blocks stride over the level's nodes; split nodes with stars partition their
-// star range into the 4 child ranges, keeping the relative order of stars
-// (stable).
-template <typename T>
-__global__ void __launch_bounds__(256) tree_partition_stars(int beg, int end, LevelRange lr,
+// Blocks of NT threads stride over the level's nodes; split nodes with stars
+// partition their star range into the 4 child ranges, keeping the relative
+// order of stars (stable). The top levels, a few nodes holding many stars each,
+// take NT = 1024 (a quarter of the block-synchronised chunks), the rest 256.
+template <typename T, int NT = 256>
+__global__ void __launch_bounds__(NT) tree_partition_stars(int beg, int end, LevelRange lr,
                                                             const int* __restrict__ stop,
                                                             const int* __restrict__ split,
                                                             const T* __restrict__ cx, const T* __restrict__ cy,
@@ -205,7 +210,7 @@ __global__ void __launch_bounds__(256) tree_partition_stars(int beg, int end, Le
   lr.get(beg, end);
   if (stop && *stop) return;
   __shared__ int cnt[4];
-  __shared__ int warp_cnt[8][4];
+  __shared__ int warp_cnt[NT / 32][4];
   __shared__ int base[4];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int k = beg + blockIdx.x; k < end; k += gridDim.x) {
@@ -254,7 +259,7 @@ __global__ void __launch_bounds__(256) tree_partition_stars(int beg, int end, Le
       __syncthreads();
       if (threadIdx.x < 4) {
         int add = 0;
-        for (int ww = 0; ww < (int)(blockDim.x >> 5); ww++) add += warp_cnt[ww][threadIdx.x];
+        for (int ww = 0; ww < NT / 32; ww++) add += warp_cnt[ww][threadIdx.x];
         base[threadIdx.x] += add;
       }
       __syncthreads();
@@ -324,75 +329,141 @@ __global__ void tree_set_neighbors(int beg, int end, LevelRange lr, const T* __r
   }
 }
 
+// Level bookkeeping of a build driven on the device: level l's nodes are
+// off[l] .. off[l + 1]; lvl_n[l] is their count.
+__global__ void tree_levels_init(int* off, int* lvl_n, int nlev, int roots, int* stop, int* dstat) {
+  off[0] = 0;
+  for (int l = 1; l <= nlev + 1; l++) off[l] = roots;
+  lvl_n[0] = roots;
+  for (int l = 1; l <= nlev; l++) lvl_n[l] = 0;
+  *stop = 0;
+  dstat[0] = dstat[1] = 0;
+}
+
+// After level l's split flags are scanned: the next level holds 4 children per
+// split node. Running out of levels or of node capacity stops the build (the
+// remaining level kernels see an empty range) and raises an error bit.
+__global__ void tree_advance_level(int l, int nlev, int* off, int* lvl_n, const long long* __restrict__ nsplit_p,
+                                   int node_cap, int* stop, int* dstat) {
+  const int end = off[l + 1];
+  long long nsplit = *stop ? 0 : *nsplit_p;
+  if (nsplit > 0 && l == nlev - 1) {
+    atomicOr(&dstat[1], kErrLevelOverflow);
+    *stop = 1;
+    nsplit = 0;
+  }
+  if (end + 4 * nsplit > node_cap) {
+    atomicOr(&dstat[1], kErrNodeOverflow);
+    *stop = 1;
+    nsplit = 0;
+  }
+  off[l + 2] = end + int(4 * nsplit);
+  lvl_n[l + 1] = int(4 * nsplit);
+}
+
 // Builds the tree over `stars` (device, permuted in place into tree order).
 // Returns false on a CUDA error or a list overflow.
+//
+// The level loop runs on the device: every level kernel reads its node range
+// from the device offsets (LevelRange) on a grid sized by the most nodes the
+// level can hold (4^l), and the host reads the offsets back once per block of
+// levels (the first block covers the depth a uniform field of this size
+// reaches) instead of synchronising on every level. Node storage is reserved
+// up front; a field that needs more restores its star order and builds again
+// with twice the capacity.
 template <typename T>
 bool build_tree(TreeDev<T>& t, StarRec<T>* stars, int nstars, T root_hl, cudaStream_t s) {
-  if (!tree_reserve(t, 1024, s)) return false;
-  if (!t.tmp_stars.reserve(nstars, s)) return false;
-  if (!t.dstat.reserve(2, s)) return false;
-  tree_init_root<T><<<1, 1, 0, s>>>(t.cx.p, t.cy.p, t.hl.p, t.level.p, t.parent.p, t.child0.p, t.sbeg.p, t.scnt.p,
-                                    t.rid.p, t.n_nbr.p, t.n_sil.p, t.n_dil.p, t.lox.p, t.hix.p, t.loy.p, t.hiy.p, root_hl,
-                                    nstars);
-  IRSB_LAUNCH_CK("tree_init_root");
-  t.level_off.assign({0, 1});
-  t.levels = 0;
-  IRSB_CKR(cudaMemsetAsync(t.dstat.p, 0, 2 * sizeof(int), s));
-  int hstat[2];
-  for (int l = 0; l < kMaxLevels; l++) {
-    int beg = t.level_off[l], end = t.level_off[l + 1];
-    int nl = end - beg;
-    if (!t.split.reserve(nl, s) || !t.rank.reserve(nl + 1, s)) return false;
-    IRSB_CKR(cudaMemsetAsync(t.dstat.p, 0, sizeof(int), s));
-    int blocks = std::min(ceil_div(nl, 256), 148 * 8);
-    tree_near_count<<<blocks, 256, 0, s>>>(beg, end, LevelRange{}, t.scnt.p, t.nbr.p, t.n_nbr.p, t.split.p, t.dstat.p);
-    IRSB_LAUNCH_CK("tree_near_count");
-    if (!exclusive_scan<int>(t.split.p, nl, t.rank.p, t.scan, s)) return false;
-    long long nsplit = 0;
-    IRSB_CKR(cudaMemcpyAsync(hstat, t.dstat.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
-    IRSB_CKR(cudaMemcpyAsync(&nsplit, t.scan.sum.p, sizeof(long long), cudaMemcpyDeviceToHost, s));
-    IRSB_CKR(cudaStreamSynchronize(s));
-    if (hstat[1]) {
-      std::fprintf(stderr, "Error. Tree neighbour/interaction list overflow (code %d).\n", hstat[1]);
+  if (!t.tmp_stars.reserve(nstars, s) || !t.star_backup.reserve(nstars, s) || !t.dstat.reserve(2, s) ||
+      !t.d_off.reserve(kMaxLevels + 2, s) || !t.d_lvl_n.reserve(kMaxLevels + 1, s) || !t.d_stop.reserve(1, s))
+    return false;
+  IRSB_CKR(cudaMemcpyAsync(t.star_backup.p, stars, size_t(nstars) * sizeof(StarRec<T>), cudaMemcpyDeviceToDevice, s));
+  long long cap = std::max<long long>(t.cap, nstars + nstars / 2 + 1024);
+  int depth = 1;  // levels of a uniform field: 4^depth >= nstars
+  while (depth < kMaxLevels && (1LL << (2 * depth)) < nstars) depth++;
+  const int G = 148 * 8;
+  auto grid = [&](int l, int per_block) {
+    const long long most = l >= 15 ? (1LL << 30) : (1LL << (2 * l));
+    return int(std::max<long long>(1, std::min<long long>(ceil_div(most, (long long)per_block), G)));
+  };
+  std::vector<int> hoff(kMaxLevels + 2);
+  t.launches = 0;
+  for (int attempt = 0;; attempt++) {
+    if (cap > (1LL << 28)) {
+      std::fprintf(stderr, "Error. Tree needs more than %lld nodes.\n", 1LL << 28);
       return false;
     }
-    if (hstat[0] <= kMaxStarsDirect) {
-      // leaves of the final level
-      fill_kernel<int><<<std::max(1, ceil_div(nl, 256)), 256, 0, s>>>(t.child0.p + beg, nl, -1);
-      IRSB_LAUNCH_CK("fill child0");
-      break;
+    if (!tree_reserve(t, int(cap), s) || !t.split.reserve(cap, s) || !t.rank.reserve(cap + 1, s) ||
+        !scan_reserve(t.scan, cap, s))
+      return false;
+    if (attempt > 0)
+      IRSB_CKR(cudaMemcpyAsync(stars, t.star_backup.p, size_t(nstars) * sizeof(StarRec<T>), cudaMemcpyDeviceToDevice,
+                               s));
+    tree_init_root<T><<<1, 1, 0, s>>>(t.cx.p, t.cy.p, t.hl.p, t.level.p, t.parent.p, t.child0.p, t.sbeg.p, t.scnt.p,
+                                      t.rid.p, t.n_nbr.p, t.n_sil.p, t.n_dil.p, t.lox.p, t.hix.p, t.loy.p, t.hiy.p,
+                                      root_hl, nstars);
+    tree_levels_init<<<1, 1, 0, s>>>(t.d_off.p, t.d_lvl_n.p, kMaxLevels, 1, t.d_stop.p, t.dstat.p);
+    IRSB_LAUNCH_CK("tree_init_root");
+    t.launches += 2;
+    int l = 0, levels = -1, err = 0, block = depth + 1;
+    while (levels < 0 && l < kMaxLevels) {
+      const int lend = std::min(kMaxLevels, l + block);
+      for (; l < lend; l++) {
+        const LevelRange lr{t.d_off.p, l}, next{t.d_off.p, l + 1};
+        const int g1 = grid(l, 256);
+        tree_near_count<<<g1, 256, 0, s>>>(0, 0, lr, t.scnt.p, t.nbr.p, t.n_nbr.p, t.split.p, t.dstat.p);
+        if (!exclusive_scan_dev<int>(t.split.p, t.d_lvl_n.p + l, cap, t.rank.p, t.scan, s)) return false;
+        tree_advance_level<<<1, 1, 0, s>>>(l, kMaxLevels, t.d_off.p, t.d_lvl_n.p, t.scan.sum.p, int(cap), t.d_stop.p,
+                                           t.dstat.p);
+        tree_make_children<T><<<g1, 256, 0, s>>>(0, 0, 0, lr, t.d_stop.p, t.split.p, t.rank.p, t.cx.p, t.cy.p, t.hl.p,
+                                                 t.level.p, t.parent.p, t.child0.p, t.sbeg.p, t.scnt.p, t.rid.p,
+                                                 t.n_nbr.p, t.n_sil.p, t.n_dil.p, t.lox.p, t.hix.p, t.loy.p, t.hiy.p);
+        if (l <= 3)  // a few nodes holding many stars each
+          tree_partition_stars<T, 1024><<<grid(l, 1), 1024, 0, s>>>(0, 0, lr, t.d_stop.p, t.split.p, t.cx.p, t.cy.p,
+                                                                      t.child0.p, t.sbeg.p, t.scnt.p, stars,
+                                                                      t.tmp_stars.p);
+        else
+          tree_partition_stars<T><<<grid(l, 1), 256, 0, s>>>(0, 0, lr, t.d_stop.p, t.split.p, t.cx.p, t.cy.p,
+                                                              t.child0.p, t.sbeg.p, t.scnt.p, stars, t.tmp_stars.p);
+        tree_set_neighbors<T><<<grid(l + 1, 256), 256, 0, s>>>(0, 0, next, t.cx.p, t.cy.p, t.hl.p, t.parent.p,
+                                                               t.child0.p, t.scnt.p, t.nbr.p, t.n_nbr.p, t.sil.p,
+                                                               t.n_sil.p, t.dil.p, t.n_dil.p, t.dstat.p);
+        IRSB_LAUNCH_CK("tree level");
+        t.launches += 9;
+      }
+      int hst[2];
+      IRSB_CKR(cudaMemcpyAsync(hoff.data(), t.d_off.p, hoff.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+      IRSB_CKR(cudaMemcpyAsync(hst, t.dstat.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+      IRSB_CKR(cudaStreamSynchronize(s));
+      err = hst[1];
+      if (err) break;
+      for (int k = 0; k < l; k++)
+        if (hoff[k + 2] == hoff[k + 1]) {  // level k split nothing: its nodes are the last leaves
+          levels = k;
+          break;
+        }
+      block = 4;
     }
-    if (l + 1 >= kMaxLevels) {
+    if (err & kErrNodeOverflow) {
+      cap *= 2;
+      continue;
+    }
+    if (err & kErrLevelOverflow) {
       std::fprintf(stderr, "Error. Tree exceeded %d levels.\n", kMaxLevels);
       return false;
     }
-    int child_base = end;
-    int nnew = int(4 * nsplit);
-    if (!tree_reserve(t, end + nnew, s)) return false;
-    tree_make_children<T><<<blocks, 256, 0, s>>>(beg, end, child_base, LevelRange{}, nullptr, t.split.p, t.rank.p,
-                                                 t.cx.p, t.cy.p, t.hl.p, t.level.p, t.parent.p, t.child0.p, t.sbeg.p,
-                                                 t.scnt.p, t.rid.p, t.n_nbr.p,
-                                                 t.n_sil.p, t.n_dil.p, t.lox.p, t.hix.p, t.loy.p, t.hiy.p);
-    IRSB_LAUNCH_CK("tree_make_children");
-    tree_partition_stars<T><<<nl, 256, 0, s>>>(beg, end, LevelRange{}, nullptr, t.split.p, t.cx.p, t.cy.p, t.child0.p, t.sbeg.p, t.scnt.p,
-                                               stars, t.tmp_stars.p);
-    IRSB_LAUNCH_CK("tree_partition_stars");
-    int nb2 = std::min(ceil_div(nnew, 256), 148 * 8);
-    tree_set_neighbors<T><<<std::max(nb2, 1), 256, 0, s>>>(child_base, child_base + nnew, LevelRange{}, t.cx.p, t.cy.p, t.hl.p,
-                                                           t.parent.p, t.child0.p, t.scnt.p, t.nbr.p, t.n_nbr.p,
-                                                           t.sil.p, t.n_sil.p, t.dil.p, t.n_dil.p, t.dstat.p);
-    IRSB_LAUNCH_CK("tree_set_neighbors");
-    t.level_off.push_back(child_base + nnew);
-    t.levels++;
+    if (err) {
+      std::fprintf(stderr, "Error. Tree neighbour/interaction list overflow (code %d).\n", err);
+      return false;
+    }
+    if (levels < 0) {
+      std::fprintf(stderr, "Error. Tree exceeded %d levels.\n", kMaxLevels);
+      return false;
+    }
+    t.levels = levels;
+    t.level_off.assign(hoff.begin(), hoff.begin() + levels + 2);
+    t.num_nodes = t.level_off.back();
+    return true;
   }
-  t.num_nodes = t.level_off.back();
-  IRSB_CKR(cudaMemcpyAsync(hstat, t.dstat.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
-  IRSB_CKR(cudaStreamSynchronize(s));
-  if (hstat[1]) {
-    std::fprintf(stderr, "Error. Tree neighbour/interaction list overflow (code %d).\n", hstat[1]);
-    return false;
-  }
-  return true;
 }
 
 }  // namespace irsb
