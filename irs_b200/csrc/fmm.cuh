@@ -77,40 +77,60 @@ __global__ void fmm_p2m(int beg, int end, LevelRange lr, int p, const T* __restr
   }
 }
 
-// Parent multipoles from its 4 children (internal nodes of one level).
+// Parent multipoles from its 4 children (internal nodes of one level). One
+// warp per node in groups of p + 1 lanes (lane l of a group computes order l);
+// group g shifts children g and g + G as two independent chains, and the
+// groups' sums are added into group 0 in group order.
 template <typename T>
 __global__ void fmm_m2m(int beg, int end, LevelRange lr, int p, const T* __restrict__ cx, const T* __restrict__ cy,
                         const T* __restrict__ hl, const int* __restrict__ child0, const double* __restrict__ btab,
                         double2* mult) {
   lr.get(beg, end);
-  int lane = threadIdx.x & 31;
-  int warps = (gridDim.x * blockDim.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int P1 = p + 1;
+  const int G = 32 / P1;
+  const int g = lane / P1, l = lane - g * P1;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  const cplx<double> zero = mk(0.0, 0.0);
   for (int k = beg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < end; k += warps) {
-    int c0 = child0[k];
-    if (c0 < 0 || lane > p) continue;
-    cplx<double> acc = mk(0.0, 0.0);
-    for (int j = 0; j < 4; j++) {
-      int c = c0 + j;
-      const double2* a = mult + (size_t)c * (p + 1);
-      cplx<double> r;
-      if (lane == 0) {
-        r = ld2(a);
+    const int c0 = child0[k];
+    if (c0 < 0) continue;  // uniform over the warp
+    cplx<double> acc = zero;
+    for (int j0 = 0; j0 < 4; j0 += 2 * G) {
+      const int ja = j0 + g, jb = ja + G;
+      if (g >= G || ja >= 4) continue;
+      const bool vb = jb < 4;
+      const int ca = c0 + ja, cb = c0 + (vb ? jb : ja);
+      const double2* aa = mult + (size_t)ca * P1;
+      const double2* ab = mult + (size_t)cb * P1;
+      cplx<double> ra, rb;
+      if (l == 0) {
+        ra = ld2(aa);
+        rb = ld2(ab);
       } else {
-        double hc = hl[c];
-        cplx<double> dz = mk((double(cx[c]) - double(cx[k])) / hc, (double(cy[c]) - double(cy[k])) / hc);
-        const cplx<double> idz = cdiv(mk(1.0, 0.0), dz);
-        r = mk(0.0, 0.0);
+        const double ha = hl[ca], hb = hl[cb];
+        const cplx<double> dza = mk((double(cx[ca]) - double(cx[k])) / ha, (double(cy[ca]) - double(cy[k])) / ha);
+        const cplx<double> dzb = mk((double(cx[cb]) - double(cx[k])) / hb, (double(cy[cb]) - double(cy[k])) / hb);
+        const cplx<double> ia = cdiv(mk(1.0, 0.0), dza), ib = cdiv(mk(1.0, 0.0), dzb);
+        ra = rb = zero;
+#pragma unroll 4
         for (int i = p; i >= 1; i--) {
-          r = cadd(r, cscale(ld2(a + i), binom(btab, lane - 1, i - 1)));
-          r = cmul(r, idz);
+          const double C = binom(btab, l - 1, i - 1);
+          ra = cmul(cadd(ra, cscale(ld2(aa + i), C)), ia);
+          rb = cmul(cadd(rb, cscale(ld2(ab + i), C)), ib);
         }
-        r = csub(r, cdivr(ld2(a), double(lane)));
-        r = cmul(r, cpowi(dz, lane));
-        r = cdivr(r, double(1u << lane));
+        ra = cdivr(cmul(csub(ra, cdivr(ld2(aa), double(l))), cpowi(dza, l)), double(1u << l));
+        rb = cdivr(cmul(csub(rb, cdivr(ld2(ab), double(l))), cpowi(dzb, l)), double(1u << l));
       }
-      acc = cadd(acc, r);
+      acc = cadd(acc, ra);
+      if (vb) acc = cadd(acc, rb);
     }
-    st2(&mult[(size_t)k * (p + 1) + lane], acc);
+    for (int gg = 1; gg < G; gg++) {
+      const int src = min(l + gg * P1, 31);
+      const cplx<double> o = mk(__shfl_sync(0xffffffffu, acc.re, src), __shfl_sync(0xffffffffu, acc.im, src));
+      if (g == 0) acc = cadd(acc, o);
+    }
+    if (g == 0) st2(&mult[(size_t)k * P1 + l], acc);
   }
 }
 
@@ -118,34 +138,42 @@ __global__ void fmm_m2m(int beg, int end, LevelRange lr, int p, const T* __restr
 // then M2L over the same-level interaction list, then P2L over the
 // different-level list.
 //
-// One warp per node, split into G = 32 / (p + 1) groups of p + 1 lanes (lane
-// l of a group computes order l). The per-interaction quantities every order
-// needs (the source's reciprocal distance and the logarithms of the order-0
-// term) are computed once, interaction j (or star j) on lane j, and read by
-// the groups through shuffles; group g takes interactions g, g + G, ... and
-// the groups' sums are added into group 0 in group order (deterministic).
-// Each interaction term is evaluated with the reference's Horner ordering.
+// W warps per node (W = 1: one warp per node; W = 8: a block per node, for
+// levels with few nodes), each split into G = 32 / (p + 1) groups of p + 1
+// lanes (lane l of a group computes order l). The per-interaction quantities
+// every order needs (the source's reciprocal distance and the logarithms of
+// the order-0 term) are computed once per warp, interaction j (or star j) on
+// lane j, and read by the groups through shuffles. Group gid of the node's
+// GW = W G groups takes interactions gid + GW n (W = 1), or gid + 2 GW n and
+// gid + GW + 2 GW n as two independent chains (W = 8); the groups' sums are
+// added in group order (deterministic). Each interaction term keeps the reference's Horner
+// ordering.
 static_assert(kMaxSameLevelIL <= 32, "one lane per same-level interaction");
-template <typename T>
-__global__ void fmm_local(int beg, int end, LevelRange lr, int p, const T* __restrict__ cx, const T* __restrict__ cy,
-                          const T* __restrict__ hl, const int* __restrict__ parent, const int* __restrict__ sbeg,
-                          const int* __restrict__ scnt, const int* __restrict__ sil, const int* __restrict__ n_sil,
-                          const int* __restrict__ dil, const int* __restrict__ n_dil,
-                          const StarRec<T>* __restrict__ stars, const double* __restrict__ btab,
-                          const double2* __restrict__ mult, double2* loc) {
+template <typename T, int W = 1>
+__global__ void __launch_bounds__(256) fmm_local(int beg, int end, LevelRange lr, int p, const T* __restrict__ cx,
+                                                 const T* __restrict__ cy, const T* __restrict__ hl,
+                                                 const int* __restrict__ parent, const int* __restrict__ sbeg,
+                                                 const int* __restrict__ scnt, const int* __restrict__ sil,
+                                                 const int* __restrict__ n_sil, const int* __restrict__ dil,
+                                                 const int* __restrict__ n_dil, const StarRec<T>* __restrict__ stars,
+                                                 const double* __restrict__ btab, const double2* __restrict__ mult,
+                                                 double2* loc) {
   lr.get(beg, end);
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, w = W > 1 ? int(threadIdx.x >> 5) : 0;
   const int P1 = p + 1;
   const int G = 32 / P1;
   const int g = lane / P1, l = lane - g * P1;
   const bool grp = g < G;
-  const int warps = (gridDim.x * blockDim.x) >> 5;
+  const int GW = G * W, gid = w * G + g;
+  __shared__ double2 s_acc[W][32];
   const cplx<double> zero = mk(0.0, 0.0);
-  for (int k = beg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < end; k += warps) {
+  const int k0 = W > 1 ? beg + int(blockIdx.x) : beg + int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int kstep = W > 1 ? int(gridDim.x) : int((gridDim.x * blockDim.x) >> 5);
+  for (int k = k0; k < end; k += kstep) {
     const double ccx = cx[k], ccy = cy[k], h = hl[k];
     cplx<double> acc = zero;
-    // L2L (group 0)
-    if (g == 0) {
+    // L2L (group 0 of warp 0)
+    if (gid == 0) {
       const int pa = parent[k];
       const double2* cp = loc + (size_t)pa * P1;
       const double hp = hl[pa];
@@ -171,50 +199,84 @@ __global__ void fmm_local(int beg, int end, LevelRange lr, int p, const T* __res
       lgj = clog_(md);
       lhj = log(hf);
     }
-    for (int j0 = 0; j0 < ns; j0 += G) {
-      const int j = j0 + g;
-      const int src = j < 32 ? j : 31;
-      const int f = __shfl_sync(0xffffffffu, fj, src);
-      const cplx<double> imd = mk(__shfl_sync(0xffffffffu, imdj.re, src), __shfl_sync(0xffffffffu, imdj.im, src));
-      const cplx<double> lg = mk(__shfl_sync(0xffffffffu, lgj.re, src), __shfl_sync(0xffffffffu, lgj.im, src));
-      const double lh = __shfl_sync(0xffffffffu, lhj, src);
-      if (!grp || j >= ns) continue;
-      const double2* b = mult + (size_t)f * P1;
-      cplx<double> t = zero;
-      for (int i = p; i >= 1; i--) {  // C(l + i - 1, i - 1) is 1 for l = 0
-        t = cadd(t, cscale(ld2(b + i), binom(btab, l + i - 1, i - 1)));
-        t = cmul(t, imd);
+    if (W > 1) {  // two interactions per group and pass
+      for (int j0 = 0; j0 < ns; j0 += 2 * GW) {
+        const int ja = j0 + gid, jb = ja + GW;
+        const int sa = ja < 32 ? ja : 31, sb = jb < 32 ? jb : 31;
+        const int fa = __shfl_sync(0xffffffffu, fj, sa), fb = __shfl_sync(0xffffffffu, fj, sb);
+        const cplx<double> ia = mk(__shfl_sync(0xffffffffu, imdj.re, sa), __shfl_sync(0xffffffffu, imdj.im, sa));
+        const cplx<double> ib = mk(__shfl_sync(0xffffffffu, imdj.re, sb), __shfl_sync(0xffffffffu, imdj.im, sb));
+        const cplx<double> lga = mk(__shfl_sync(0xffffffffu, lgj.re, sa), __shfl_sync(0xffffffffu, lgj.im, sa));
+        const cplx<double> lgb = mk(__shfl_sync(0xffffffffu, lgj.re, sb), __shfl_sync(0xffffffffu, lgj.im, sb));
+        const double lha = __shfl_sync(0xffffffffu, lhj, sa), lhb = __shfl_sync(0xffffffffu, lhj, sb);
+        if (!grp || ja >= ns) continue;
+        const bool vb = jb < ns;
+        const double2* ba = mult + (size_t)fa * P1;
+        const double2* bb = mult + (size_t)(vb ? fb : fa) * P1;
+        cplx<double> ta = zero, tb = zero;
+#pragma unroll 4
+        for (int i = p; i >= 1; i--) {  // C(l + i - 1, i - 1) is 1 for l = 0
+          const double C = binom(btab, l + i - 1, i - 1);
+          ta = cmul(cadd(ta, cscale(ld2(ba + i), C)), ia);
+          tb = cmul(cadd(tb, cscale(ld2(bb + i), C)), ib);
+        }
+        const cplx<double> b0a = ld2(ba), b0b = ld2(bb);
+        if (l == 0) {
+          ta = cadd(cadd(ta, cmul(b0a, lga)), cscale(b0a, lha));
+          tb = cadd(cadd(tb, cmul(b0b, lgb)), cscale(b0b, lhb));
+        } else {
+          ta = cmul(csub(ta, cdivr(b0a, double(l))), cpowi(cneg(ia), l));  // 1 / dz^l
+          tb = cmul(csub(tb, cdivr(b0b, double(l))), cpowi(cneg(ib), l));
+        }
+        acc = cadd(acc, ta);
+        if (vb) acc = cadd(acc, tb);
       }
-      const cplx<double> b0 = ld2(b);
-      if (l == 0) {
-        t = cadd(t, cmul(b0, lg));
-        t = cadd(t, cscale(b0, lh));
-      } else {
-        t = csub(t, cdivr(b0, double(l)));
-        t = cmul(t, cpowi(cneg(imd), l));  // 1 / dz^l
+    } else {  // one interaction per group and pass (fewer registers, more warps resident)
+      for (int j0 = 0; j0 < ns; j0 += G) {
+        const int j = j0 + g;
+        const int src = j < 32 ? j : 31;
+        const int f = __shfl_sync(0xffffffffu, fj, src);
+        const cplx<double> imd = mk(__shfl_sync(0xffffffffu, imdj.re, src), __shfl_sync(0xffffffffu, imdj.im, src));
+        const cplx<double> lg = mk(__shfl_sync(0xffffffffu, lgj.re, src), __shfl_sync(0xffffffffu, lgj.im, src));
+        const double lh = __shfl_sync(0xffffffffu, lhj, src);
+        if (!grp || j >= ns) continue;
+        const double2* b = mult + (size_t)f * P1;
+        cplx<double> t = zero;
+        for (int i = p; i >= 1; i--) {
+          t = cadd(t, cscale(ld2(b + i), binom(btab, l + i - 1, i - 1)));
+          t = cmul(t, imd);
+        }
+        const cplx<double> b0 = ld2(b);
+        if (l == 0) {
+          t = cadd(t, cmul(b0, lg));
+          t = cadd(t, cscale(b0, lh));
+        } else {
+          t = csub(t, cdivr(b0, double(l)));
+          t = cmul(t, cpowi(cneg(imd), l));
+        }
+        acc = cadd(acc, t);
       }
-      acc = cadd(acc, t);
     }
     // P2L: star u of each list's chunk of 32: 1 / dz and log(-dz) on lane u
     const int nd = n_dil[k];
     const double lhk = nd > 0 ? log(h) : 0.0;
     for (int q = 0; q < nd; q++) {
       const int f = dil[k * kMaxDiffLevelIL + q];
-      const int sb = sbeg[f], sn = scnt[f];
+      const int sb0 = sbeg[f], sn = scnt[f];
       cplx<double> t = zero;
       for (int i0 = 0; i0 < sn; i0 += 32) {
         cplx<double> idu = zero, lgu = zero;
         double mu = 0.0;
         if (i0 + lane < sn) {
-          const StarRec<T> st = stars[sb + i0 + lane];
+          const StarRec<T> st = stars[sb0 + i0 + lane];
           const cplx<double> d = mk((double(st.x) - ccx) / h, (double(st.y) - ccy) / h);
           mu = double(st.m);
           idu = cdiv(mk(1.0, 0.0), d);
           lgu = clog_(cneg(d));
         }
         const int cnt = min(32, sn - i0);
-        for (int u0 = 0; u0 < cnt; u0 += G) {
-          const int u = u0 + g;
+        for (int u0 = 0; u0 < cnt; u0 += GW) {
+          const int u = u0 + gid;
           const int src = u < 32 ? u : 31;
           const cplx<double> id = mk(__shfl_sync(0xffffffffu, idu.re, src), __shfl_sync(0xffffffffu, idu.im, src));
           const cplx<double> lg = mk(__shfl_sync(0xffffffffu, lgu.re, src), __shfl_sync(0xffffffffu, lgu.im, src));
@@ -231,13 +293,23 @@ __global__ void fmm_local(int beg, int end, LevelRange lr, int p, const T* __res
       }
       acc = cadd(acc, t);
     }
-    // the groups' sums into group 0, in group order
+    // the groups' sums into group 0 of the warp, then the warps' into warp 0
     for (int gg = 1; gg < G; gg++) {
       const int src = min(l + gg * P1, 31);
       const cplx<double> o = mk(__shfl_sync(0xffffffffu, acc.re, src), __shfl_sync(0xffffffffu, acc.im, src));
       if (g == 0) acc = cadd(acc, o);
     }
-    if (g == 0) st2(&loc[(size_t)k * P1 + l], acc);
+    if (W > 1) {
+      if (g == 0) s_acc[w][l] = make_double2(acc.re, acc.im);
+      __syncthreads();
+      if (w == 0 && g == 0) {
+        for (int ww = 1; ww < W; ww++) acc = cadd(acc, ld2(&s_acc[ww][l]));
+        st2(&loc[(size_t)k * P1 + l], acc);
+      }
+      __syncthreads();
+    } else if (g == 0) {
+      st2(&loc[(size_t)k * P1 + l], acc);
+    }
   }
 }
 
@@ -271,8 +343,14 @@ bool compute_fmm(FmmDev& f, TreeDev<T>& t, const StarRec<T>* stars, int p, cudaS
     int beg = t.level_off[l], end = t.level_off[l + 1];
     int nw = end - beg;
     int blocks = std::max(1, std::min(ceil_div(nw, 8), 148 * 16));
-    fmm_local<T><<<blocks, 256, 0, s>>>(beg, end, LevelRange{}, p, t.cx.p, t.cy.p, t.hl.p, t.parent.p, t.sbeg.p, t.scnt.p,
-                                        t.sil.p, t.n_sil.p, t.dil.p, t.n_dil.p, stars, f.btab.p, f.mult.p, f.loc.p);
+    if (nw <= 512)  // few nodes: a block of 8 warps per node
+      fmm_local<T, 8><<<std::max(1, std::min(nw, 148 * 16)), 256, 0, s>>>(
+          beg, end, LevelRange{}, p, t.cx.p, t.cy.p, t.hl.p, t.parent.p, t.sbeg.p, t.scnt.p, t.sil.p, t.n_sil.p,
+          t.dil.p, t.n_dil.p, stars, f.btab.p, f.mult.p, f.loc.p);
+    else
+      fmm_local<T><<<blocks, 256, 0, s>>>(beg, end, LevelRange{}, p, t.cx.p, t.cy.p, t.hl.p, t.parent.p, t.sbeg.p,
+                                          t.scnt.p, t.sil.p, t.n_sil.p, t.dil.p, t.n_dil.p, stars, f.btab.p, f.mult.p,
+                                          f.loc.p);
     IRSB_LAUNCH_CK("fmm_local");
   }
   return true;

@@ -67,6 +67,7 @@ struct TreeDev {
   ScanScratch scan;
   DevVec<StarRec<T>> tmp_stars, star_backup;
   DevVec<int> d_off, d_lvl_n, d_stop;  // level offsets and sizes on the device
+  DevVec<int> chunk_cnt;               // per-chunk key counts of the wide partition
   long long launches = 0;              // kernels the last build launched
 };
 
@@ -269,6 +270,143 @@ __global__ void __launch_bounds__(NT) tree_partition_stars(int beg, int end, Lev
   }
 }
 
+// The same stable partition for the first two levels, whose NN nodes (1 or 4)
+// hold every star between them, on many blocks: the stars are cut into chunks
+// of kPartChunk; a star's key is its node's index in the level times 4 plus its
+// quadrant (0 in a node that does not split). Count per chunk and key, scan
+// each key over the chunks (stable), scatter, copy back. A level that is
+// absent (the root did not split) is left alone.
+constexpr int kPartChunk = 1024;
+
+template <typename T, int NN>
+__device__ __forceinline__ int wide_key(int i, int beg, const int* __restrict__ split, const T* __restrict__ cx,
+                                        const T* __restrict__ cy, const int* __restrict__ sbeg,
+                                        const int* __restrict__ scnt, const StarRec<T>& st) {
+  int j = 0;
+#pragma unroll
+  for (int jj = 1; jj < NN; jj++)
+    if (i >= sbeg[beg + jj]) j = jj;  // the level's nodes are consecutive star ranges in node order
+  const int k = beg + j;
+  return 4 * j + (split[j] ? star_quadrant(st.x, st.y, cx[k], cy[k]) : 0);
+}
+
+template <int NN>
+__device__ __forceinline__ bool wide_level(LevelRange lr, const int* stop, int& beg) {
+  int b = 0, e = 0;
+  lr.get(b, e);
+  beg = b;
+  return !(stop && *stop) && e - b == NN;
+}
+
+template <typename T, int NN>
+__global__ void __launch_bounds__(256) tree_wide_count(LevelRange lr, const int* __restrict__ stop,
+                                                       const int* __restrict__ split, const T* __restrict__ cx,
+                                                       const T* __restrict__ cy, const int* __restrict__ sbeg,
+                                                       const int* __restrict__ scnt,
+                                                       const StarRec<T>* __restrict__ stars, int nstars, int* cnt) {
+  int beg;
+  if (!wide_level<NN>(lr, stop, beg)) return;
+  __shared__ int c[4 * NN];
+  if (threadIdx.x < 4 * NN) c[threadIdx.x] = 0;
+  __syncthreads();
+  const int i0 = blockIdx.x * kPartChunk, i1 = min(i0 + kPartChunk, nstars);
+  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x)
+    atomicAdd(&c[wide_key<T, NN>(i, beg, split, cx, cy, sbeg, scnt, stars[i])], 1);
+  __syncthreads();
+  if (threadIdx.x < 4 * NN) cnt[blockIdx.x * 4 * NN + threadIdx.x] = c[threadIdx.x];
+}
+
+// One block: per key, the exclusive scan over the chunks plus the key's base
+// (its node's first star plus the counts of the node's lower quadrants); the
+// children's star ranges.
+template <int NN>
+__global__ void tree_wide_offsets(LevelRange lr, const int* __restrict__ stop, const int* __restrict__ split,
+                                  const int* __restrict__ child0, int* sbeg, int* scnt, int nchunks, int* cnt) {
+  int beg;
+  if (!wide_level<NN>(lr, stop, beg)) return;
+  constexpr int K = 4 * NN;
+  __shared__ int tot[K], base[K];
+  if (threadIdx.x < K) {
+    int run = 0;
+    for (int c = 0; c < nchunks; c++) {
+      const int v = cnt[c * K + threadIdx.x];
+      cnt[c * K + threadIdx.x] = run;
+      run += v;
+    }
+    tot[threadIdx.x] = run;
+  }
+  __syncthreads();
+  if (threadIdx.x < NN) {
+    const int j = threadIdx.x, k = beg + j;
+    int acc = sbeg[k];
+    for (int q = 0; q < 4; q++) {
+      base[4 * j + q] = acc;
+      if (split[j]) {
+        sbeg[child0[k] + q] = acc;
+        scnt[child0[k] + q] = tot[4 * j + q];
+      }
+      acc += tot[4 * j + q];
+    }
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < nchunks * K; idx += blockDim.x) cnt[idx] += base[idx % K];
+}
+
+template <typename T, int NN>
+__global__ void __launch_bounds__(256) tree_wide_scatter(LevelRange lr, const int* __restrict__ stop,
+                                                         const int* __restrict__ split, const T* __restrict__ cx,
+                                                         const T* __restrict__ cy, const int* __restrict__ sbeg,
+                                                         const int* __restrict__ scnt,
+                                                         const StarRec<T>* __restrict__ stars, int nstars,
+                                                         const int* __restrict__ off, StarRec<T>* __restrict__ tmp) {
+  int beg;
+  if (!wide_level<NN>(lr, stop, beg)) return;
+  constexpr int K = 4 * NN;
+  __shared__ int run[K];
+  __shared__ int wc[8][K];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x < K) run[threadIdx.x] = off[blockIdx.x * K + threadIdx.x];
+  __syncthreads();
+  const int i0 = blockIdx.x * kPartChunk, i1 = min(i0 + kPartChunk, nstars);
+  for (int r = i0; r < i1; r += 256) {  // rounds in star order
+    const int i = r + threadIdx.x;
+    int key = -1;
+    StarRec<T> st;
+    if (i < i1) {
+      st = stars[i];
+      key = wide_key<T, NN>(i, beg, split, cx, cy, sbeg, scnt, st);
+    }
+    unsigned mine = 0;
+#pragma unroll
+    for (int kk = 0; kk < K; kk++) {
+      const unsigned m = __ballot_sync(0xffffffffu, key == kk);
+      if (lane == 0) wc[w][kk] = __popc(m);
+      if (key == kk) mine = m;
+    }
+    __syncthreads();
+    if (key >= 0) {
+      int pos = run[key];
+      for (int ww = 0; ww < w; ww++) pos += wc[ww][key];
+      tmp[pos + __popc(mine & ((1u << lane) - 1u))] = st;
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+      int add = 0;
+      for (int ww = 0; ww < 8; ww++) add += wc[ww][threadIdx.x];
+      run[threadIdx.x] += add;
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T, int NN>
+__global__ void tree_wide_copy(LevelRange lr, const int* __restrict__ stop, int nstars,
+                               const StarRec<T>* __restrict__ tmp, StarRec<T>* __restrict__ stars) {
+  int beg;
+  if (!wide_level<NN>(lr, stop, beg)) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nstars; i += gridDim.x * blockDim.x) stars[i] = tmp[i];
+}
+
 // set_neighbors (tree_node.cuh:183-267) for the nodes of one level (>= 1).
 template <typename T>
 __global__ void tree_set_neighbors(int beg, int end, LevelRange lr, const T* __restrict__ cx,
@@ -361,6 +499,18 @@ __global__ void tree_advance_level(int l, int nlev, int* off, int* lvl_n, const 
   lvl_n[l + 1] = int(4 * nsplit);
 }
 
+template <typename T, int NN>
+bool wide_partition(TreeDev<T>& t, LevelRange lr, StarRec<T>* stars, int nstars, int nchunks, cudaStream_t s) {
+  tree_wide_count<T, NN><<<nchunks, 256, 0, s>>>(lr, t.d_stop.p, t.split.p, t.cx.p, t.cy.p, t.sbeg.p, t.scnt.p, stars,
+                                                nstars, t.chunk_cnt.p);
+  tree_wide_offsets<NN><<<1, 256, 0, s>>>(lr, t.d_stop.p, t.split.p, t.child0.p, t.sbeg.p, t.scnt.p, nchunks,
+                                          t.chunk_cnt.p);
+  tree_wide_scatter<T, NN><<<nchunks, 256, 0, s>>>(lr, t.d_stop.p, t.split.p, t.cx.p, t.cy.p, t.sbeg.p, t.scnt.p,
+                                                  stars, nstars, t.chunk_cnt.p, t.tmp_stars.p);
+  tree_wide_copy<T, NN><<<std::min(nchunks * 4, 148 * 8), 256, 0, s>>>(lr, t.d_stop.p, nstars, t.tmp_stars.p, stars);
+  return IRSB_CK(cudaGetLastError());
+}
+
 // Builds the tree over `stars` (device, permuted in place into tree order).
 // Returns false on a CUDA error or a list overflow.
 //
@@ -376,6 +526,8 @@ bool build_tree(TreeDev<T>& t, StarRec<T>* stars, int nstars, T root_hl, cudaStr
   if (!t.tmp_stars.reserve(nstars, s) || !t.star_backup.reserve(nstars, s) || !t.dstat.reserve(2, s) ||
       !t.d_off.reserve(kMaxLevels + 2, s) || !t.d_lvl_n.reserve(kMaxLevels + 1, s) || !t.d_stop.reserve(1, s))
     return false;
+  const int nchunks = std::max(1, ceil_div(nstars, kPartChunk));
+  if (!t.chunk_cnt.reserve(size_t(nchunks) * 16, s)) return false;
   IRSB_CKR(cudaMemcpyAsync(t.star_backup.p, stars, size_t(nstars) * sizeof(StarRec<T>), cudaMemcpyDeviceToDevice, s));
   long long cap = std::max<long long>(t.cap, nstars + nstars / 2 + 1024);
   int depth = 1;  // levels of a uniform field: 4^depth >= nstars
@@ -417,7 +569,13 @@ bool build_tree(TreeDev<T>& t, StarRec<T>* stars, int nstars, T root_hl, cudaStr
         tree_make_children<T><<<g1, 256, 0, s>>>(0, 0, 0, lr, t.d_stop.p, t.split.p, t.rank.p, t.cx.p, t.cy.p, t.hl.p,
                                                  t.level.p, t.parent.p, t.child0.p, t.sbeg.p, t.scnt.p, t.rid.p,
                                                  t.n_nbr.p, t.n_sil.p, t.n_dil.p, t.lox.p, t.hix.p, t.loy.p, t.hiy.p);
-        if (l <= 3)  // a few nodes holding many stars each
+        if (l == 0) {  // the root: every star, on many blocks
+          if (!wide_partition<T, 1>(t, lr, stars, nstars, nchunks, s)) return false;
+          t.launches += 3;
+        } else if (l == 1) {  // the root's 4 children: every star
+          if (!wide_partition<T, 4>(t, lr, stars, nstars, nchunks, s)) return false;
+          t.launches += 3;
+        } else if (l <= 3)  // a few nodes holding many stars each
           tree_partition_stars<T, 1024><<<grid(l, 1), 1024, 0, s>>>(0, 0, lr, t.d_stop.p, t.split.p, t.cx.p, t.cy.p,
                                                                       t.child0.p, t.sbeg.p, t.scnt.p, stars,
                                                                       t.tmp_stars.p);
