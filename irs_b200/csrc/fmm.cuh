@@ -134,6 +134,17 @@ __global__ void fmm_m2m(int beg, int end, LevelRange lr, int p, const T* __restr
   }
 }
 
+// Powers of z within each group of P1 lanes: lane l of a group returns z^l
+// (z^0 = 1), by a product scan over the group (log2(P1) steps).
+__device__ __forceinline__ cplx<double> group_powers(cplx<double> z, int l, int P1) {
+  cplx<double> v = l == 0 ? mk(1.0, 0.0) : z;
+  for (int o = 1; o < P1; o <<= 1) {
+    const cplx<double> u = mk(__shfl_up_sync(0xffffffffu, v.re, o), __shfl_up_sync(0xffffffffu, v.im, o));
+    if (l >= o) v = cmul(u, v);
+  }
+  return v;
+}
+
 // Local coefficients of the nodes of one level (>= 2): L2L from the parent,
 // then M2L over the same-level interaction list, then P2L over the
 // different-level list.
@@ -143,11 +154,17 @@ __global__ void fmm_m2m(int beg, int end, LevelRange lr, int p, const T* __restr
 // lanes (lane l of a group computes order l). The per-interaction quantities
 // every order needs (the source's reciprocal distance and the logarithms of
 // the order-0 term) are computed once per warp, interaction j (or star j) on
-// lane j, and read by the groups through shuffles. Group gid of the node's
-// GW = W G groups takes interactions gid + GW n (W = 1), or gid + 2 GW n and
-// gid + GW + 2 GW n as two independent chains (W = 8); the groups' sums are
-// added in group order (deterministic). Each interaction term keeps the reference's Horner
-// ordering.
+// lane j, and read by the groups through shuffles; group gid of the node's
+// GW = W G groups takes interactions gid, gid + GW, ... and the groups' sums
+// are added in group order (deterministic).
+//
+// M2L as a weighted sum: with w = 1 / (-dz) and u_k = b_k w^k (lane k of the
+// group forms u_k, its power w^k by a product scan over the group),
+//   c_0 = sum_k u_k + b_0 log(-dz) + b_0 log(hl_from),
+//   c_l = (sum_k C(l + k - 1, k - 1) u_k - b_0 / l) (-w)^l,
+// the same quantity as the reference's Horner form (fmm.cuh:281-322), with
+// real weights: two FMAs per term instead of a complex product. P2L takes its
+// powers (1 / dz)^l from the same scan.
 static_assert(kMaxSameLevelIL <= 32, "one lane per same-level interaction");
 template <typename T, int W = 1>
 __global__ void __launch_bounds__(256) fmm_local(int beg, int end, LevelRange lr, int p, const T* __restrict__ cx,
@@ -159,13 +176,14 @@ __global__ void __launch_bounds__(256) fmm_local(int beg, int end, LevelRange lr
                                                  const double* __restrict__ btab, const double2* __restrict__ mult,
                                                  double2* loc) {
   lr.get(beg, end);
-  const int lane = threadIdx.x & 31, w = W > 1 ? int(threadIdx.x >> 5) : 0;
+  const int lane = threadIdx.x & 31, ws = threadIdx.x >> 5, w = W > 1 ? ws : 0;
   const int P1 = p + 1;
   const int G = 32 / P1;
-  const int g = lane / P1, l = lane - g * P1;
+  const int g = lane / P1, l = lane - g * P1, gb = g * P1;
   const bool grp = g < G;
   const int GW = G * W, gid = w * G + g;
   __shared__ double2 s_acc[W][32];
+  __shared__ double2 s_u[8][32];  // per warp: u_k of each group's interaction
   const cplx<double> zero = mk(0.0, 0.0);
   const int k0 = W > 1 ? beg + int(blockIdx.x) : beg + int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int kstep = W > 1 ? int(gridDim.x) : int((gridDim.x * blockDim.x) >> 5);
@@ -199,60 +217,36 @@ __global__ void __launch_bounds__(256) fmm_local(int beg, int end, LevelRange lr
       lgj = clog_(md);
       lhj = log(hf);
     }
-    if (W > 1) {  // two interactions per group and pass
-      for (int j0 = 0; j0 < ns; j0 += 2 * GW) {
-        const int ja = j0 + gid, jb = ja + GW;
-        const int sa = ja < 32 ? ja : 31, sb = jb < 32 ? jb : 31;
-        const int fa = __shfl_sync(0xffffffffu, fj, sa), fb = __shfl_sync(0xffffffffu, fj, sb);
-        const cplx<double> ia = mk(__shfl_sync(0xffffffffu, imdj.re, sa), __shfl_sync(0xffffffffu, imdj.im, sa));
-        const cplx<double> ib = mk(__shfl_sync(0xffffffffu, imdj.re, sb), __shfl_sync(0xffffffffu, imdj.im, sb));
-        const cplx<double> lga = mk(__shfl_sync(0xffffffffu, lgj.re, sa), __shfl_sync(0xffffffffu, lgj.im, sa));
-        const cplx<double> lgb = mk(__shfl_sync(0xffffffffu, lgj.re, sb), __shfl_sync(0xffffffffu, lgj.im, sb));
-        const double lha = __shfl_sync(0xffffffffu, lhj, sa), lhb = __shfl_sync(0xffffffffu, lhj, sb);
-        if (!grp || ja >= ns) continue;
-        const bool vb = jb < ns;
-        const double2* ba = mult + (size_t)fa * P1;
-        const double2* bb = mult + (size_t)(vb ? fb : fa) * P1;
-        cplx<double> ta = zero, tb = zero;
-#pragma unroll 4
-        for (int i = p; i >= 1; i--) {  // C(l + i - 1, i - 1) is 1 for l = 0
-          const double C = binom(btab, l + i - 1, i - 1);
-          ta = cmul(cadd(ta, cscale(ld2(ba + i), C)), ia);
-          tb = cmul(cadd(tb, cscale(ld2(bb + i), C)), ib);
-        }
-        const cplx<double> b0a = ld2(ba), b0b = ld2(bb);
-        if (l == 0) {
-          ta = cadd(cadd(ta, cmul(b0a, lga)), cscale(b0a, lha));
-          tb = cadd(cadd(tb, cmul(b0b, lgb)), cscale(b0b, lhb));
-        } else {
-          ta = cmul(csub(ta, cdivr(b0a, double(l))), cpowi(cneg(ia), l));  // 1 / dz^l
-          tb = cmul(csub(tb, cdivr(b0b, double(l))), cpowi(cneg(ib), l));
-        }
-        acc = cadd(acc, ta);
-        if (vb) acc = cadd(acc, tb);
-      }
-    } else {  // one interaction per group and pass (fewer registers, more warps resident)
-      for (int j0 = 0; j0 < ns; j0 += G) {
-        const int j = j0 + g;
-        const int src = j < 32 ? j : 31;
-        const int f = __shfl_sync(0xffffffffu, fj, src);
-        const cplx<double> imd = mk(__shfl_sync(0xffffffffu, imdj.re, src), __shfl_sync(0xffffffffu, imdj.im, src));
-        const cplx<double> lg = mk(__shfl_sync(0xffffffffu, lgj.re, src), __shfl_sync(0xffffffffu, lgj.im, src));
-        const double lh = __shfl_sync(0xffffffffu, lhj, src);
-        if (!grp || j >= ns) continue;
-        const double2* b = mult + (size_t)f * P1;
+    for (int j0 = 0; j0 < ns; j0 += GW) {
+      const int j = j0 + gid;
+      const int src = j < 32 ? j : 31;
+      const int f = __shfl_sync(0xffffffffu, fj, src);
+      const cplx<double> imd = mk(__shfl_sync(0xffffffffu, imdj.re, src), __shfl_sync(0xffffffffu, imdj.im, src));
+      const cplx<double> lg = mk(__shfl_sync(0xffffffffu, lgj.re, src), __shfl_sync(0xffffffffu, lgj.im, src));
+      const double lh = __shfl_sync(0xffffffffu, lhj, src);
+      const bool valid = grp && j < ns;
+      const cplx<double> pw = group_powers(imd, l, P1);  // w^l
+      const cplx<double> bl = valid ? ld2(mult + (size_t)f * P1 + l) : zero;
+      const cplx<double> u = l == 0 ? bl : cmul(bl, pw);
+      __syncwarp();
+      s_u[ws][lane] = make_double2(u.re, u.im);
+      __syncwarp();
+      if (valid) {
         cplx<double> t = zero;
-        for (int i = p; i >= 1; i--) {
-          t = cadd(t, cscale(ld2(b + i), binom(btab, l + i - 1, i - 1)));
-          t = cmul(t, imd);
+        for (int kk = p; kk >= 1; kk--) {  // C(l + k - 1, k - 1) is 1 for l = 0
+          const double C = binom(btab, l + kk - 1, kk - 1);
+          const double2 uk = s_u[ws][gb + kk];
+          t.re = fma(C, uk.x, t.re);
+          t.im = fma(C, uk.y, t.im);
         }
-        const cplx<double> b0 = ld2(b);
+        const double2 b0v = s_u[ws][gb];
+        const cplx<double> b0 = mk(b0v.x, b0v.y);
         if (l == 0) {
           t = cadd(t, cmul(b0, lg));
           t = cadd(t, cscale(b0, lh));
         } else {
           t = csub(t, cdivr(b0, double(l)));
-          t = cmul(t, cpowi(cneg(imd), l));
+          t = cmul(t, (l & 1) ? cneg(pw) : pw);  // 1 / dz^l = (-w)^l
         }
         acc = cadd(acc, t);
       }
@@ -281,13 +275,13 @@ __global__ void __launch_bounds__(256) fmm_local(int beg, int end, LevelRange lr
           const cplx<double> id = mk(__shfl_sync(0xffffffffu, idu.re, src), __shfl_sync(0xffffffffu, idu.im, src));
           const cplx<double> lg = mk(__shfl_sync(0xffffffffu, lgu.re, src), __shfl_sync(0xffffffffu, lgu.im, src));
           const double m = __shfl_sync(0xffffffffu, mu, src);
+          const cplx<double> pw = group_powers(id, l, P1);  // (1 / d)^l
           if (!grp || u >= cnt) continue;
           if (l == 0) {
             t = cadd(t, cscale(lg, m));
             t.re += m * lhk;
           } else {
-            // m / (l d^l) = (m / l) (1/d)^l
-            t = csub(t, cscale(cpowi(id, l), m / double(l)));
+            t = csub(t, cscale(pw, m / double(l)));  // m / (l d^l)
           }
         }
       }
