@@ -158,13 +158,17 @@ __device__ __forceinline__ cplx<double> group_powers(cplx<double> z, int l, int 
 // GW = W G groups takes interactions gid, gid + GW, ... and the groups' sums
 // are added in group order (deterministic).
 //
-// M2L as a weighted sum: with w = 1 / (-dz) and u_k = b_k w^k (lane k of the
-// group forms u_k, its power w^k by a product scan over the group),
-//   c_0 = sum_k u_k + b_0 log(-dz) + b_0 log(hl_from),
-//   c_l = (sum_k C(l + k - 1, k - 1) u_k - b_0 / l) (-w)^l,
-// the same quantity as the reference's Horner form (fmm.cuh:281-322), with
-// real weights: two FMAs per term instead of a complex product. P2L takes its
-// powers (1 / dz)^l from the same scan.
+// Each translation is a binomial-weighted sum over scaled coefficients, with
+// the powers from a product scan over the group (lane k holds z^k) and the
+// binomial weights of lane l staged once per block in shared memory:
+//   M2L, w = 1 / (-dz), u_k = b_k w^k (fmm.cuh:281-322):
+//     c_0 = sum_k u_k + b_0 log(-dz) + b_0 log(hl_from),
+//     c_l = (sum_k C(l + k - 1, k - 1) u_k - b_0 / l) (-w)^l;
+//   L2L, v_i = c_i dz^i (fmm.cuh:204-223):
+//     d_l = sum_{i >= 1} C(i, l) v_i (1 / dz)^l 2^-l;
+//   P2L: -m / (l d^l) with (1 / d)^l from the scan.
+// The same quantities as the reference's Horner forms, with real weights (two
+// FMAs per term) and the divisions by l, dz^l and 2^l as products.
 static_assert(kMaxSameLevelIL <= 32, "one lane per same-level interaction");
 template <typename T, int W = 1>
 __global__ void __launch_bounds__(256) fmm_local(int beg, int end, LevelRange lr, int p, const T* __restrict__ cx,
@@ -182,27 +186,44 @@ __global__ void __launch_bounds__(256) fmm_local(int beg, int end, LevelRange lr
   const int g = lane / P1, l = lane - g * P1, gb = g * P1;
   const bool grp = g < G;
   const int GW = G * W, gid = w * G + g;
+  const double inv_l = l > 0 ? 1.0 / double(l) : 0.0;
+  const double inv_2l = 1.0 / double(1u << (l & 31));  // exact
   __shared__ double2 s_acc[W][32];
-  __shared__ double2 s_u[8][32];  // per warp: u_k of each group's interaction
+  __shared__ double2 s_u[8][32];   // per warp: the scaled coefficients of each group's term
+  __shared__ double s_wm[32][32];  // [k][lane]: C(l + k - 1, k - 1) (M2L)
+  __shared__ double s_wl[32][32];  // [i][lane]: C(i, l) (L2L)
+  for (int idx = threadIdx.x; idx < 32 * 32; idx += blockDim.x) {
+    const int kk = idx >> 5, ln = idx & 31, ll = ln - (ln / P1) * P1;
+    s_wm[kk][ln] = kk >= 1 && kk <= p ? binom(btab, ll + kk - 1, kk - 1) : 0.0;
+    s_wl[kk][ln] = kk >= 1 && kk <= p ? binom(btab, kk, ll) : 0.0;
+  }
+  __syncthreads();
   const cplx<double> zero = mk(0.0, 0.0);
   const int k0 = W > 1 ? beg + int(blockIdx.x) : beg + int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int kstep = W > 1 ? int(gridDim.x) : int((gridDim.x * blockDim.x) >> 5);
   for (int k = k0; k < end; k += kstep) {
     const double ccx = cx[k], ccy = cy[k], h = hl[k];
     cplx<double> acc = zero;
-    // L2L (group 0 of warp 0)
-    if (gid == 0) {
+    // L2L (every group of warp 0 forms it; group 0 keeps it)
+    if (w == 0) {
       const int pa = parent[k];
-      const double2* cp = loc + (size_t)pa * P1;
       const double hp = hl[pa];
       const cplx<double> dz = mk((ccx - double(cx[pa])) / hp, (ccy - double(cy[pa])) / hp);
+      const cplx<double> pz = group_powers(dz, l, P1);
+      const cplx<double> pi = group_powers(cdiv(mk(1.0, 0.0), dz), l, P1);
+      const cplx<double> v = cmul(ld2(loc + (size_t)pa * P1 + l), pz);
+      __syncwarp();
+      s_u[ws][lane] = make_double2(v.re, v.im);
+      __syncwarp();
       cplx<double> r = zero;
+#pragma unroll 4
       for (int i = p; i >= 1; i--) {
-        r = cadd(r, cscale(ld2(cp + i), binom(btab, i, l)));
-        r = cmul(r, dz);
+        const double C = s_wl[i][lane];
+        const double2 vi = s_u[ws][gb + i];
+        r.re = fma(C, vi.x, r.re);
+        r.im = fma(C, vi.y, r.im);
       }
-      r = cdiv(r, cpowi(dz, l));
-      acc = cdivr(r, double(1u << l));
+      if (g == 0) acc = cscale(cmul(r, pi), inv_2l);
     }
     // M2L: interaction j's source, 1 / (-dz), log(-dz) and log(hl_from) on lane j
     const int ns = n_sil[k];
@@ -233,8 +254,9 @@ __global__ void __launch_bounds__(256) fmm_local(int beg, int end, LevelRange lr
       __syncwarp();
       if (valid) {
         cplx<double> t = zero;
+#pragma unroll 4
         for (int kk = p; kk >= 1; kk--) {  // C(l + k - 1, k - 1) is 1 for l = 0
-          const double C = binom(btab, l + kk - 1, kk - 1);
+          const double C = s_wm[kk][lane];
           const double2 uk = s_u[ws][gb + kk];
           t.re = fma(C, uk.x, t.re);
           t.im = fma(C, uk.y, t.im);
@@ -245,7 +267,7 @@ __global__ void __launch_bounds__(256) fmm_local(int beg, int end, LevelRange lr
           t = cadd(t, cmul(b0, lg));
           t = cadd(t, cscale(b0, lh));
         } else {
-          t = csub(t, cdivr(b0, double(l)));
+          t = csub(t, cscale(b0, inv_l));
           t = cmul(t, (l & 1) ? cneg(pw) : pw);  // 1 / dz^l = (-w)^l
         }
         acc = cadd(acc, t);
@@ -281,7 +303,7 @@ __global__ void __launch_bounds__(256) fmm_local(int beg, int end, LevelRange lr
             t = cadd(t, cscale(lg, m));
             t.re += m * lhk;
           } else {
-            t = csub(t, cscale(pw, m / double(l)));  // m / (l d^l)
+            t = csub(t, cscale(pw, m * inv_l));  // m / (l d^l)
           }
         }
       }
