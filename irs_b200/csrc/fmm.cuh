@@ -12,15 +12,19 @@
 //        c_l = (sum_k b_k C(l+k-1,k-1)/(-dz)^k - b_0/l) / dz^l       fmm.cuh:281-322
 //   P2L  dz = (z_i - c_to)/hl_to,
 //        c_0 = sum m_i (log(-dz) + log(hl_to)), c_l = -sum m_i/(l dz^l) fmm.cuh:387-413
-// evaluated with the reference's Horner ordering, dividing by dz through one
-// reciprocal per interaction (FP64 throughout). Level schedule as
+// evaluated in FP64 as binomial-weighted sums of scaled coefficients (each
+// power z^k from a product scan over a group of lanes, each division by l,
+// dz^l or 2^l as a product): the reference's quantities, summed in another
+// order than its Horner form (the coefficients agree to rounding). Level
+// schedule as
 // include/ipm.cuh:874-901: P2M+M2M bottom-up, then L2L, M2L, P2L top-down from
 // level 2. The reference builds an int binomial table, which overflows beyond
 // order ~17 (binomial_coefficients.cuh:11-44); this table is int64, exact up to
 // row 62, and is used as double.
 //
 // Layout: coefficients of node k, order l at [k * (p + 1) + l] as double2.
-// Kernel shape: one warp per node, lane l computes order l (p <= 31).
+// Kernel shape: one warp (or, for levels of few nodes, one block) per node, in
+// groups of p + 1 lanes, lane l of a group computing order l (p <= 31).
 #pragma once
 #include "common.cuh"
 #include "devutil.cuh"
@@ -50,90 +54,6 @@ __device__ __forceinline__ double binom(const double* tab, int n, int k) {
   return tab[n * (n + 1) / 2 + k];
 }
 
-template <typename T>
-__global__ void fmm_p2m(int beg, int end, LevelRange lr, int p, const T* __restrict__ cx, const T* __restrict__ cy,
-                        const T* __restrict__ hl, const int* __restrict__ child0, const int* __restrict__ sbeg,
-                        const int* __restrict__ scnt, const StarRec<T>* __restrict__ stars, double2* mult) {
-  lr.get(beg, end);
-  int lane = threadIdx.x & 31;
-  int warps = (gridDim.x * blockDim.x) >> 5;
-  for (int k = beg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < end; k += warps) {
-    if (child0[k] >= 0 || scnt[k] == 0) continue;
-    if (lane > p) continue;
-    double ccx = cx[k], ccy = cy[k], h = hl[k];
-    int b = sbeg[k], n = scnt[k];
-    cplx<double> r = mk(0.0, 0.0);
-    for (int i = 0; i < n; i++) {
-      StarRec<T> s = stars[b + i];
-      if (lane == 0) {
-        r.re += double(s.m);
-      } else {
-        cplx<double> d = mk((double(s.x) - ccx) / h, (double(s.y) - ccy) / h);
-        r = csub(r, cscale(cpowi(d, lane), double(s.m)));
-      }
-    }
-    if (lane > 0) r = cdivr(r, double(lane));
-    st2(&mult[(size_t)k * (p + 1) + lane], r);
-  }
-}
-
-// Parent multipoles from its 4 children (internal nodes of one level). One
-// warp per node in groups of p + 1 lanes (lane l of a group computes order l);
-// group g shifts children g and g + G as two independent chains, and the
-// groups' sums are added into group 0 in group order.
-template <typename T>
-__global__ void fmm_m2m(int beg, int end, LevelRange lr, int p, const T* __restrict__ cx, const T* __restrict__ cy,
-                        const T* __restrict__ hl, const int* __restrict__ child0, const double* __restrict__ btab,
-                        double2* mult) {
-  lr.get(beg, end);
-  const int lane = threadIdx.x & 31;
-  const int P1 = p + 1;
-  const int G = 32 / P1;
-  const int g = lane / P1, l = lane - g * P1;
-  const int warps = (gridDim.x * blockDim.x) >> 5;
-  const cplx<double> zero = mk(0.0, 0.0);
-  for (int k = beg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < end; k += warps) {
-    const int c0 = child0[k];
-    if (c0 < 0) continue;  // uniform over the warp
-    cplx<double> acc = zero;
-    for (int j0 = 0; j0 < 4; j0 += 2 * G) {
-      const int ja = j0 + g, jb = ja + G;
-      if (g >= G || ja >= 4) continue;
-      const bool vb = jb < 4;
-      const int ca = c0 + ja, cb = c0 + (vb ? jb : ja);
-      const double2* aa = mult + (size_t)ca * P1;
-      const double2* ab = mult + (size_t)cb * P1;
-      cplx<double> ra, rb;
-      if (l == 0) {
-        ra = ld2(aa);
-        rb = ld2(ab);
-      } else {
-        const double ha = hl[ca], hb = hl[cb];
-        const cplx<double> dza = mk((double(cx[ca]) - double(cx[k])) / ha, (double(cy[ca]) - double(cy[k])) / ha);
-        const cplx<double> dzb = mk((double(cx[cb]) - double(cx[k])) / hb, (double(cy[cb]) - double(cy[k])) / hb);
-        const cplx<double> ia = cdiv(mk(1.0, 0.0), dza), ib = cdiv(mk(1.0, 0.0), dzb);
-        ra = rb = zero;
-#pragma unroll 4
-        for (int i = p; i >= 1; i--) {
-          const double C = binom(btab, l - 1, i - 1);
-          ra = cmul(cadd(ra, cscale(ld2(aa + i), C)), ia);
-          rb = cmul(cadd(rb, cscale(ld2(ab + i), C)), ib);
-        }
-        ra = cdivr(cmul(csub(ra, cdivr(ld2(aa), double(l))), cpowi(dza, l)), double(1u << l));
-        rb = cdivr(cmul(csub(rb, cdivr(ld2(ab), double(l))), cpowi(dzb, l)), double(1u << l));
-      }
-      acc = cadd(acc, ra);
-      if (vb) acc = cadd(acc, rb);
-    }
-    for (int gg = 1; gg < G; gg++) {
-      const int src = min(l + gg * P1, 31);
-      const cplx<double> o = mk(__shfl_sync(0xffffffffu, acc.re, src), __shfl_sync(0xffffffffu, acc.im, src));
-      if (g == 0) acc = cadd(acc, o);
-    }
-    if (g == 0) st2(&mult[(size_t)k * P1 + l], acc);
-  }
-}
-
 // Powers of z within each group of P1 lanes: lane l of a group returns z^l
 // (z^0 = 1), by a product scan over the group (log2(P1) steps).
 __device__ __forceinline__ cplx<double> group_powers(cplx<double> z, int l, int P1) {
@@ -143,6 +63,117 @@ __device__ __forceinline__ cplx<double> group_powers(cplx<double> z, int l, int 
     if (l >= o) v = cmul(u, v);
   }
   return v;
+}
+
+// Multipoles of the leaves of one level from their stars. One warp per leaf in
+// groups of p + 1 lanes (lane l of a group computes order l); group g takes
+// stars g, g + G, ... with the star's powers ((z - c) / hl)^l from a product
+// scan over the group, and the groups' sums are added in group order.
+template <typename T>
+__global__ void fmm_p2m(int beg, int end, LevelRange lr, int p, const T* __restrict__ cx, const T* __restrict__ cy,
+                        const T* __restrict__ hl, const int* __restrict__ child0, const int* __restrict__ sbeg,
+                        const int* __restrict__ scnt, const StarRec<T>* __restrict__ stars, double2* mult) {
+  lr.get(beg, end);
+  const int lane = threadIdx.x & 31;
+  const int P1 = p + 1;
+  const int G = 32 / P1;
+  const int g = lane / P1, l = lane - g * P1;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int k = beg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < end; k += warps) {
+    if (child0[k] >= 0 || scnt[k] == 0) continue;  // uniform over the warp
+    const double ccx = cx[k], ccy = cy[k], h = hl[k];
+    const int b = sbeg[k], n = scnt[k];
+    cplx<double> r = mk(0.0, 0.0);
+    for (int i0 = 0; i0 < n; i0 += G) {
+      const int i = i0 + g;
+      const bool valid = g < G && i < n;
+      const StarRec<T> st = stars[b + (valid ? i : 0)];
+      const cplx<double> d = mk((double(st.x) - ccx) / h, (double(st.y) - ccy) / h);
+      const cplx<double> pw = group_powers(d, l, P1);
+      if (!valid) continue;
+      if (l == 0) r.re += double(st.m);
+      else r = csub(r, cscale(pw, double(st.m)));
+    }
+    for (int gg = 1; gg < G; gg++) {
+      const int src = min(l + gg * P1, 31);
+      const cplx<double> o = mk(__shfl_sync(0xffffffffu, r.re, src), __shfl_sync(0xffffffffu, r.im, src));
+      if (g == 0) r = cadd(r, o);
+    }
+    if (g == 0) st2(&mult[(size_t)k * P1 + l], l > 0 ? cdivr(r, double(l)) : r);
+  }
+}
+
+// Parent multipoles from its 4 children (internal nodes of one level). One
+// warp per node in groups of p + 1 lanes (lane l of a group computes order l);
+// group g shifts children g, g + G, ... and the groups' sums are added into
+// group 0 in group order. Each shift is a binomial-weighted sum: with
+// u_i = a_i (1 / dz)^i (lane i, its power from a product scan over the group),
+//   b_0 = a_0,  b_l = (sum_i C(l - 1, i - 1) u_i - a_0 / l) dz^l 2^-l,
+// the reference's quantity (fmm.cuh:109-139) with real weights, staged per
+// block in shared memory.
+template <typename T>
+__global__ void __launch_bounds__(256) fmm_m2m(int beg, int end, LevelRange lr, int p, const T* __restrict__ cx,
+                                               const T* __restrict__ cy, const T* __restrict__ hl,
+                                               const int* __restrict__ child0, const double* __restrict__ btab,
+                                               double2* mult) {
+  lr.get(beg, end);
+  const int lane = threadIdx.x & 31, ws = threadIdx.x >> 5;
+  const int P1 = p + 1;
+  const int G = 32 / P1;
+  const int g = lane / P1, l = lane - g * P1, gb = g * P1;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  const double inv_l = l > 0 ? 1.0 / double(l) : 0.0;
+  const double inv_2l = 1.0 / double(1u << (l & 31));  // exact
+  __shared__ double2 s_u[8][32];
+  __shared__ double s_w[32][32];  // [i][lane]: C(l - 1, i - 1)
+  for (int idx = threadIdx.x; idx < 32 * 32; idx += blockDim.x) {
+    const int i = idx >> 5, ln = idx & 31, ll = ln - (ln / P1) * P1;
+    s_w[i][ln] = i >= 1 && i <= p ? binom(btab, ll - 1, i - 1) : 0.0;
+  }
+  __syncthreads();
+  const cplx<double> zero = mk(0.0, 0.0);
+  for (int k = beg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < end; k += warps) {
+    const int c0 = child0[k];
+    if (c0 < 0) continue;  // uniform over the warp
+    cplx<double> acc = zero;
+    for (int j0 = 0; j0 < 4; j0 += G) {
+      const int j = j0 + g;
+      const bool valid = g < G && j < 4;
+      const int c = c0 + (valid ? j : 0);
+      const double hc = hl[c];
+      const cplx<double> dz = mk((double(cx[c]) - double(cx[k])) / hc, (double(cy[c]) - double(cy[k])) / hc);
+      const cplx<double> pz = group_powers(dz, l, P1);
+      const cplx<double> pi = group_powers(cdiv(mk(1.0, 0.0), dz), l, P1);
+      const cplx<double> al = ld2(mult + (size_t)c * P1 + l);
+      const cplx<double> u = l == 0 ? al : cmul(al, pi);
+      __syncwarp();
+      s_u[ws][lane] = make_double2(u.re, u.im);
+      __syncwarp();
+      if (!valid) continue;
+      cplx<double> r;
+      if (l == 0) {
+        r = al;
+      } else {
+        r = zero;
+#pragma unroll 4
+        for (int i = p; i >= 1; i--) {
+          const double C = s_w[i][lane];
+          const double2 ui = s_u[ws][gb + i];
+          r.re = fma(C, ui.x, r.re);
+          r.im = fma(C, ui.y, r.im);
+        }
+        const double2 a0 = s_u[ws][gb];
+        r = cscale(cmul(csub(r, cscale(mk(a0.x, a0.y), inv_l)), pz), inv_2l);
+      }
+      acc = cadd(acc, r);
+    }
+    for (int gg = 1; gg < G; gg++) {
+      const int src = min(l + gg * P1, 31);
+      const cplx<double> o = mk(__shfl_sync(0xffffffffu, acc.re, src), __shfl_sync(0xffffffffu, acc.im, src));
+      if (g == 0) acc = cadd(acc, o);
+    }
+    if (g == 0) st2(&mult[(size_t)k * P1 + l], acc);
+  }
 }
 
 // Local coefficients of the nodes of one level (>= 2): L2L from the parent,
