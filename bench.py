@@ -10,13 +10,15 @@ Default workload (the plain-IPM case at its stated substitute shear):
 One step = the whole device pipeline on the star field resident in HBM:
 quadtree build, FP64 expansions, leaf records, lattice lens equation and the
 fixed-point deposition. value = pixels of all steps / device time (CUDA events,
-max over ranks). e2e = the same through the C ABI with host buffers: the star
-field is copied from host memory, run() executes the full pipeline (including
-histograms) and the map is copied back, timed on the host clock.
+max over ranks). e2e = the same through the public API with host buffers: per
+step, IPM.run() copies the star field from host memory, runs the full pipeline
+(including the histograms) and returns the map as a numpy array in host memory
+(IPM.magnifications), timed on the host clock.
 
---impl reference times the reference algorithm on the host CPU cores (the
-oracle's FMM form with four lens evaluations per cell and the reference polygon
-deposition, OpenMP), on a bounded band of cells, scaled to the full lattice.
+--impl reference times the reference's own IPM on the host CPU cores (its tree,
+expansions and cell-shooting kernel compiled for the host, OpenMP; the oracle's
+restatement where that library was not built), the tree once per step and a
+band of cell rows scaled to the full lattice.
 Under torchrun every rank runs an independent replica (the map of one
 realisation is not sharded here); value sums the replicas.
 """
@@ -570,13 +572,12 @@ def our_arm(args):
     # to within the sampling noise of its mean mass; the geometry does not use it
     e.safety_scale = 1.3
     e.set_stars(stars, rectangular=False, corner=(m.value("rad"), 0.0), theta_star=m.theta_star)
-    for _ in range(max(1, args.warmup // 2)):
+    for _ in range(args.warmup):
         e.run()
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        e.run()
-        _ = e.magnifications.sum()
+        e.run()  # the step's result: e.magnifications, a host array
     barrier()
     e2e_time = time.perf_counter() - t0
     if dist is not None:

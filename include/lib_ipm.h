@@ -114,6 +114,8 @@ void set_shoot_launch(IPMHandle* self, int threads, int ctas_per_sm); /* FP32 le
 int get_shoot_threads(IPMHandle* self);
 int get_shoot_ctas_per_sm(IPMHandle* self);
 bool copy_maps_device(IPMHandle* self, void* total, void* minima, void* saddles); /* integer maps to device buffers */
+/* the last run's map (0 total, 1 minima, 2 saddles) into dst[num_pixels_y2][num_pixels_y1], several host threads */
+bool copy_pixels(IPMHandle* self, int which, IPM_DTYPE* dst);
 bool derive(IPMHandle* self);                          /* validate + derived parameters, no GPU work */
 double get_value(IPMHandle* self, const char* name);   /* derived / run-time value by name, NaN if unknown */
 /* diagnostics: copies of internal device state */

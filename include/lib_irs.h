@@ -106,6 +106,8 @@ void set_shoot_launch(IRSHandle* self, int threads, int ctas_per_sm); /* FP32 le
 int get_shoot_threads(IRSHandle* self);
 int get_shoot_ctas_per_sm(IRSHandle* self);
 bool copy_maps_device(IRSHandle* self, void* total, void* minima, void* saddles); /* integer maps to device buffers */
+/* the last run's map (0 total, 1 minima, 2 saddles) into dst[num_pixels_y2][num_pixels_y1], several host threads */
+bool copy_pixels(IRSHandle* self, int which, int* dst);
 bool derive(IRSHandle* self);
 double get_value(IRSHandle* self, const char* name);
 int get_tree_num_nodes(IRSHandle* self);

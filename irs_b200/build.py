@@ -31,6 +31,7 @@ NVCC_FLAGS = ARCH + [
     "-O3",
     "-lineinfo",
     "-Xcompiler", "-fPIC",
+    "-Xcompiler", "-fopenmp",  # host-side copies of the maps
     "-shared",
     "--expt-relaxed-constexpr",
 ]
@@ -75,7 +76,7 @@ def build_one(name: str, defs, force: bool = False, extra=None, source: str = "c
     if not force and not _stale(out):
         return out
     cmd = [nvcc()] + NVCC_FLAGS + list(defs) + list(extra or []) + [
-        "-I", CSRC, os.path.join(CSRC, source), "-o", out + ".tmp", "-lcurand"]
+        "-I", CSRC, os.path.join(CSRC, source), "-o", out + ".tmp", "-lcurand", "-lgomp"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
@@ -91,7 +92,7 @@ def build_exe(name: str, defs, force: bool = False, source: str = "cli.cu") -> s
         return out
     flags = [f for f in NVCC_FLAGS if f not in ("-shared",)]
     cmd = [nvcc()] + flags + list(defs) + ["-I", CSRC, os.path.join(CSRC, source), "-o", out + ".tmp",
-                                            "-lcurand"]
+                                            "-lcurand", "-lgomp"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)

@@ -22,7 +22,9 @@
 #include "stars.cuh"
 #include "tree.cuh"
 
+#include <algorithm>
 #include <chrono>
+#include <cstring>
 #include <fstream>
 #include <iostream>
 #include <string>
@@ -155,6 +157,22 @@ class MapMaker {
   }
 
   Pix* pixels() { return h_pix.p; }
+  // The map of the last run (0 total, 1 minima, 2 saddles) copied into dst
+  // (npix values) by the OpenMP threads (a persistent pool: no thread start
+  // per call); false if that map does not exist.
+  bool copy_pixels(int which, Pix* dst) const {
+    const Pix* src = which == 0 ? h_pix.p : (have_parities ? (which == 1 ? h_pmin.p : h_psad.p) : nullptr);
+    if (!src || !dst || which < 0 || which > 2) return false;
+    const long long n = (long long)prm.num_pixels_y.re * prm.num_pixels_y.im;
+    const long long chunk = 1 << 18;
+    const long long nchunk = (n + chunk - 1) / chunk;
+#pragma omp parallel for schedule(static) num_threads(8) if (nchunk > 1)
+    for (long long c = 0; c < nchunk; c++) {
+      const long long a = c * chunk, b = std::min(n, a + chunk);
+      std::memcpy(dst + a, src + a, size_t(b - a) * sizeof(Pix));
+    }
+    return true;
+  }
   Pix* pixels_minima() { return have_parities ? h_pmin.p : nullptr; }
   Pix* pixels_saddles() { return have_parities ? h_psad.p : nullptr; }
   T* stars_ptr() { return stars_out.empty() ? nullptr : &stars_out[0].x; }
@@ -213,6 +231,7 @@ class MapMaker {
     // stars in tree order, as the reference leaves them
     IRSB_CKR(cudaMemcpyAsync(stars_out.data(), d_stars_.p, size_t(n) * sizeof(StarRec<T>), cudaMemcpyDeviceToHost,
                              stream_));
+    n_hist_ = 0;
     if (!verts_only && !post(verbose)) return false;
     IRSB_CKR(cudaStreamSynchronize(stream_));
     if (verbose >= 1) {
@@ -282,6 +301,7 @@ class MapMaker {
 
   // Writes the reference's output files (include/ipm.cuh:1122-1322).
   bool save(int verbose) {
+    if (!fetch_hists()) return false;
     const Params<T>& p = prm;
     const std::string pre = p.outfile_prefix + (IS_IRS ? "irs_" : "ipm_");
     {
@@ -455,6 +475,14 @@ class MapMaker {
  private:
   cudaStream_t stream_ = nullptr;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, ev2_ = nullptr;
+  struct HistSlot {
+    DevVec<int> dev;
+    std::vector<int>* out = nullptr;
+    int len = 0;
+  };
+  static constexpr int kMaxHists = 6;  // linear and log10, of the total, minima and saddle maps
+  HistSlot hist_slots_[kMaxHists];
+  int n_hist_ = 0;
   cudaEvent_t ev_lat0_ = nullptr, ev_lat1_ = nullptr, ev_dep1_ = nullptr;
   DevVec<StarRec<T>> d_stars_;
   TreeDev<T> tree_;
@@ -468,7 +496,6 @@ class MapMaker {
   DevVec<double2> d_verts_;
   DevVec<unsigned long long> d_red_;
   DevVec<long long> d_mm_;
-  DevVec<int> d_hist_;
 
   bool init_stream() {
     if (stream_) return true;
@@ -717,16 +744,37 @@ class MapMaker {
     return true;
   }
 
+  // Histogram of a device map, counted on the device and kept there: `out`
+  // is filled by fetch_hists() when save() writes it (the histograms are not
+  // otherwise read), so run() does not copy them back.
   template <typename V>
   bool make_hist(const V* v, long long n, int hmin, int len, int factor, int use_log, std::vector<int>& out) {
-    if (!d_hist_.alloc_exact(len)) return false;
-    IRSB_CKR(cudaMemsetAsync(d_hist_.p, 0, size_t(len) * sizeof(int), stream_));
-    int g = int(std::max<long long>(1, std::min<long long>((n + 255) / 256, 148LL * 8)));
-    histogram_map<V><<<g, 256, 0, stream_>>>(v, n, hmin, len, factor, use_log, d_hist_.p);
+    if (n_hist_ >= kMaxHists) return false;
+    HistSlot& h = hist_slots_[n_hist_++];
+    if (!h.dev.alloc_exact(len)) return false;
+    IRSB_CKR(cudaMemsetAsync(h.dev.p, 0, size_t(len) * sizeof(int), stream_));
+    if (len <= kHistSmemBins) {
+      int g = int(std::max<long long>(1, std::min<long long>((n + 1023) / 1024, 148LL)));
+      histogram_map_smem<V><<<g, 1024, size_t(len) * sizeof(int), stream_>>>(v, n, hmin, len, factor, use_log,
+                                                                            h.dev.p);
+    } else {
+      int g = int(std::max<long long>(1, std::min<long long>((n + 255) / 256, 148LL * 8)));
+      histogram_map<V><<<g, 256, 0, stream_>>>(v, n, hmin, len, factor, use_log, h.dev.p);
+    }
     IRSB_LAUNCH_CK("histogram_map");
-    out.resize(len);
-    IRSB_CKR(cudaMemcpyAsync(out.data(), d_hist_.p, size_t(len) * sizeof(int), cudaMemcpyDeviceToHost, stream_));
-    IRSB_CKR(cudaStreamSynchronize(stream_));
+    h.out = &out;
+    h.len = len;
+    return true;
+  }
+  // device histograms of the last run -> result vectors
+  bool fetch_hists() {
+    for (int i = 0; i < n_hist_; i++) {
+      HistSlot& h = hist_slots_[i];
+      h.out->resize(h.len);
+      if (!IRSB_CK(cudaMemcpy(h.out->data(), h.dev.p, size_t(h.len) * sizeof(int), cudaMemcpyDeviceToHost)))
+        return false;
+    }
+    n_hist_ = 0;
     return true;
   }
 

@@ -64,22 +64,56 @@ __global__ void minmax_nonneg(const V* __restrict__ v, long long n, typename Ord
 // histogram[round(v * factor - hmin)]++ ; log form uses log10(v). Values whose
 // bin falls outside [0, len) (log10 of an empty pixel) are not counted.
 template <typename V>
+__device__ __forceinline__ long long hist_bin(V v, int hmin, int len, int factor, int use_log) {
+  double x;
+  if constexpr (std::is_floating_point<V>::value) {
+    if (use_log) {
+      V lv = log10(v);
+      x = round(double(V(lv * factor - hmin)));
+    } else {
+      x = round(1.0 * v * factor - hmin);
+    }
+  } else {
+    x = round(1.0 * v * factor - hmin);
+  }
+  return (x >= 0 && x < len) ? (long long)x : -1;
+}
+
+// One warp-uniform pass over the map: lanes that fall in the same bin are
+// matched (neighbouring pixels mostly do) and their leader adds their count
+// with one atomic.
+template <typename V, typename Add>
+__device__ __forceinline__ void hist_pass(const V* __restrict__ v, long long n, int hmin, int len, int factor,
+                                          int use_log, Add add) {
+  const int lane = threadIdx.x & 31;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long base = (blockIdx.x * (long long)blockDim.x + threadIdx.x) - lane; base < n; base += stride) {
+    const long long k = base + lane;
+    const long long b = k < n ? hist_bin<V>(v[k], hmin, len, factor, use_log) : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, b);
+    if (b >= 0 && lane == __ffs(peers) - 1) add(b, __popc(peers));
+  }
+}
+
+template <typename V>
 __global__ void histogram_map(const V* __restrict__ v, long long n, int hmin, int len, int factor, int use_log,
                               int* __restrict__ hist) {
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-    double x;
-    if constexpr (std::is_floating_point<V>::value) {
-      if (use_log) {
-        V lv = log10(v[k]);
-        x = round(double(V(lv * factor - hmin)));
-      } else {
-        x = round(1.0 * v[k] * factor - hmin);
-      }
-    } else {
-      x = round(1.0 * v[k] * factor - hmin);
-    }
-    if (x >= 0 && x < len) atomicAdd(&hist[(long long)x], 1);
-  }
+  hist_pass<V>(v, n, hmin, len, factor, use_log, [&](long long b, int c) { atomicAdd(&hist[b], c); });
+}
+
+// The same for histograms of at most kHistSmemBins bins: each block counts in
+// shared memory, then adds its non-zero bins to the global histogram.
+constexpr int kHistSmemBins = 12288;
+template <typename V>
+__global__ void histogram_map_smem(const V* __restrict__ v, long long n, int hmin, int len, int factor,
+                                   int use_log, int* __restrict__ hist) {
+  extern __shared__ int sh[];
+  for (int i = threadIdx.x; i < len; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
+  hist_pass<V>(v, n, hmin, len, factor, use_log, [&](long long b, int c) { atomicAdd(&sh[b], c); });
+  __syncthreads();
+  for (int i = threadIdx.x; i < len; i += blockDim.x)
+    if (sh[i]) atomicAdd(&hist[i], sh[i]);
 }
 
 }  // namespace irsb

@@ -465,19 +465,24 @@ class _MapMaker:
     def corner(self):
         return (self.lib.get_corner_x1(self.obj), self.lib.get_corner_x2(self.obj))
 
-    def _map(self, getter):
-        ptr = getter(self.obj)
+    def _map(self, which):
+        """A numpy copy of the last run's map (0 total, 1 minima, 2 saddles),
+        filled by the library's multi-threaded copy; None if it does not exist."""
+        ptr = getattr(self.lib, ("get_pixels", "get_pixels_minima", "get_pixels_saddles")[which])(self.obj)
         if not ptr:
             return None
-        return np.ctypeslib.as_array(ptr, shape=(self.num_pixels_y2, self.num_pixels_y1)).copy()
+        out = np.empty((self.num_pixels_y2, self.num_pixels_y1), dtype=ptr._type_)
+        if not self.lib.copy_pixels(self.obj, which, out.ctypes.data_as(C.POINTER(ptr._type_))):
+            raise Exception(f"Error copying the {self._label} map")
+        return out
 
     def run(self):
         if not self.lib.run(self.obj, self.verbose):
             raise Exception(f"Error running {self._label}")
-        self.magnifications = self._map(self.lib.get_pixels)
+        self.magnifications = self._map(0)
         if self.write_parities:
-            self.magnifications_minima = self._map(self.lib.get_pixels_minima)
-            self.magnifications_saddles = self._map(self.lib.get_pixels_saddles)
+            self.magnifications_minima = self._map(1)
+            self.magnifications_saddles = self._map(2)
         else:
             self.magnifications_minima = None
             self.magnifications_saddles = None
