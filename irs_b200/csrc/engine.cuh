@@ -203,8 +203,10 @@ class MapMaker {
     if (!d_stars_.alloc_exact(n)) return false;
     // ---- star field
     if (from_stars) {
-      const StarRec<T>* src = file_stars.data();
-      IRSB_CKR(cudaMemcpyAsync(d_stars_.p, src, size_t(n) * sizeof(StarRec<T>), cudaMemcpyHostToDevice, stream_));
+      // the host copy is the field itself: no read-back before the moments
+      stars_out.swap(file_stars);
+      IRSB_CKR(cudaMemcpyAsync(d_stars_.p, stars_out.data(), size_t(n) * sizeof(StarRec<T>), cudaMemcpyHostToDevice,
+                               stream_));
       p.random_seed = 0;
     } else {
       while (p.random_seed == 0)
@@ -213,11 +215,11 @@ class MapMaker {
       generate_stars_kernel<T><<<blocks, 256, 0, stream_>>>(d_stars_.p, n, p.random_seed, p.rectangular, p.corner,
                                                             p.mf_kind, p.m_lower, p.m_upper, p.m_solar);
       IRSB_LAUNCH_CK("generate_stars_kernel");
+      stars_out.resize(n);
+      IRSB_CKR(cudaMemcpyAsync(stars_out.data(), d_stars_.p, size_t(n) * sizeof(StarRec<T>), cudaMemcpyDeviceToHost,
+                               stream_));
+      IRSB_CKR(cudaStreamSynchronize(stream_));
     }
-    stars_out.resize(n);
-    IRSB_CKR(cudaMemcpyAsync(stars_out.data(), d_stars_.p, size_t(n) * sizeof(StarRec<T>), cudaMemcpyDeviceToHost,
-                             stream_));
-    IRSB_CKR(cudaStreamSynchronize(stream_));
     star_field_moments<T>(n, p.rectangular, p.corner, p.theta_star, stars_out.data(), p.kappa_star_actual,
                           p.m_lower_actual, p.m_upper_actual, p.mean_mass_actual, p.mean_mass2_actual,
                           p.mean_mass2_ln_mass_actual);
@@ -226,7 +228,7 @@ class MapMaker {
     if (use_host_stars) p.starfile = "";
     prm = p;
 
-    launches = 1;  // star generation
+    launches = from_stars ? 0 : 1;  // star generation
     if (!device_pipeline()) return false;
     // stars in tree order, as the reference leaves them
     IRSB_CKR(cudaMemcpyAsync(stars_out.data(), d_stars_.p, size_t(n) * sizeof(StarRec<T>), cudaMemcpyDeviceToHost,
