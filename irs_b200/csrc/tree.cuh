@@ -467,6 +467,81 @@ __global__ void tree_set_neighbors(int beg, int end, LevelRange lr, const T* __r
   }
 }
 
+// The same lists with one warp per node: lane q examines candidate q in the
+// order of the loops above (the 4 siblings, then for each of the parent's
+// neighbours either the neighbour itself, a leaf, or its 4 children), and
+// each list takes its candidates in that order through a ballot prefix, so
+// the lists are identical to the one-thread form.
+template <typename T>
+__global__ void tree_set_neighbors_warp(LevelRange lr, const T* __restrict__ cx, const T* __restrict__ cy,
+                                        const T* __restrict__ hl, const int* __restrict__ parent,
+                                        const int* __restrict__ child0, const int* __restrict__ scnt, int* nbr,
+                                        int* n_nbr, int* sil, int* n_sil, int* dil, int* n_dil, int* dstat) {
+  int beg = 0, end = 0;
+  lr.get(beg, end);
+  const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int k = beg + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < end; k += warps) {
+    const int p = parent[k];
+    const T h = hl[k], x = cx[k], y = cy[k];
+    const int pc0 = child0[p];
+    const int nq = 4 + 4 * n_nbr[p];
+    int nn = 0, ns = 0, nd = 0, err = 0;
+    for (int q0 = 0; q0 < nq; q0 += 32) {
+      const int q = q0 + lane;
+      int cat = 0, c = -1;  // 1 neighbour, 2 same-level interaction, 3 different-level interaction
+      if (q < 4) {
+        c = pc0 + q;
+        if (scnt[c] != 0 && c != k) cat = 1;
+      } else if (q < nq) {
+        const int i = (q - 4) >> 2, j = (q - 4) & 3;
+        const int nb = nbr[p * kMaxNeighbors + i];
+        if (scnt[nb] != 0) {
+          const int nc0 = child0[nb];
+          if (nc0 < 0) {
+            if (j == 0) {
+              c = nb;
+              cat = (double(xfabs(T(cx[nb] - x))) < 3.5 * double(h) && double(xfabs(T(cy[nb] - y))) < 3.5 * double(h))
+                        ? 1
+                        : 3;
+            }
+          } else {
+            c = nc0 + j;
+            if (scnt[c] != 0) cat = (xfabs(T(cx[c] - x)) < 3 * h && xfabs(T(cy[c] - y)) < 3 * h) ? 1 : 2;
+          }
+        }
+      }
+      const unsigned m1 = __ballot_sync(0xffffffffu, cat == 1);
+      const unsigned m2 = __ballot_sync(0xffffffffu, cat == 2);
+      const unsigned m3 = __ballot_sync(0xffffffffu, cat == 3);
+      if (cat == 1) {
+        const int pos = nn + __popc(m1 & below);
+        if (pos < kMaxNeighbors) nbr[k * kMaxNeighbors + pos] = c;
+        else err |= kErrNeighborOverflow;
+      } else if (cat == 2) {
+        const int pos = ns + __popc(m2 & below);
+        if (pos < kMaxSameLevelIL) sil[k * kMaxSameLevelIL + pos] = c;
+        else err |= kErrSameLevelOverflow;
+      } else if (cat == 3) {
+        const int pos = nd + __popc(m3 & below);
+        if (pos < kMaxDiffLevelIL) dil[k * kMaxDiffLevelIL + pos] = c;
+        else err |= kErrDiffLevelOverflow;
+      }
+      nn += __popc(m1);
+      ns += __popc(m2);
+      nd += __popc(m3);
+    }
+    err = __reduce_or_sync(0xffffffffu, unsigned(err));
+    if (lane == 0) {
+      n_nbr[k] = min(nn, kMaxNeighbors);
+      n_sil[k] = min(ns, kMaxSameLevelIL);
+      n_dil[k] = min(nd, kMaxDiffLevelIL);
+      if (err) atomicOr(&dstat[1], err);
+    }
+  }
+}
+
 // Level bookkeeping of a build driven on the device: level l's nodes are
 // off[l] .. off[l + 1]; lvl_n[l] is their count.
 __global__ void tree_levels_init(int* off, int* lvl_n, int nlev, int roots, int* stop, int* dstat) {
@@ -582,9 +657,9 @@ bool build_tree(TreeDev<T>& t, StarRec<T>* stars, int nstars, T root_hl, cudaStr
         else
           tree_partition_stars<T><<<grid(l, 1), 256, 0, s>>>(0, 0, lr, t.d_stop.p, t.split.p, t.cx.p, t.cy.p,
                                                               t.child0.p, t.sbeg.p, t.scnt.p, stars, t.tmp_stars.p);
-        tree_set_neighbors<T><<<grid(l + 1, 256), 256, 0, s>>>(0, 0, next, t.cx.p, t.cy.p, t.hl.p, t.parent.p,
-                                                               t.child0.p, t.scnt.p, t.nbr.p, t.n_nbr.p, t.sil.p,
-                                                               t.n_sil.p, t.dil.p, t.n_dil.p, t.dstat.p);
+        tree_set_neighbors_warp<T><<<grid(l + 1, 8), 256, 0, s>>>(next, t.cx.p, t.cy.p, t.hl.p, t.parent.p,
+                                                                  t.child0.p, t.scnt.p, t.nbr.p, t.n_nbr.p, t.sil.p,
+                                                                  t.n_sil.p, t.dil.p, t.n_dil.p, t.dstat.p);
         IRSB_LAUNCH_CK("tree level");
         t.launches += 9;
       }
