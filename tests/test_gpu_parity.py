@@ -62,6 +62,41 @@ def test_tree_structure_and_coefficients(gpu, dbl):
     assert np.abs(gl - ol).max() <= tol * scale_l
 
 
+def test_tree_rebuild_after_node_overflow(gpu):
+    """Four clusters of stars 1e-6 of the field radius across need about 3300
+    tree nodes, more than the build reserves at first (1.5 per star + 1024):
+    the build restores the star order, reserves twice as many and builds again.
+    The tree must equal the oracle's exactly."""
+    a = irs_b200.IRS(**IRS_SMALL, is_double=True)
+    a.derive()
+    n = int(a.value("num_stars"))
+    R = float(np.hypot(a.value("corner_x1"), a.value("corner_x2")))
+    rng = np.random.default_rng(5)
+    ang = 2 * np.pi * rng.random(4)
+    cen = R * 0.6 * np.sqrt(rng.random(4))[:, None] * np.stack([np.cos(ang), np.sin(ang)], 1)
+    per = n // 4
+    pts = np.concatenate([cen[i] + 1e-6 * R * rng.standard_normal((per, 2)) for i in range(4)] +
+                         [R * 0.5 * (rng.random((n - 4 * per, 2)) - 0.5)])
+    stars = np.concatenate([pts, np.ones((n, 1))], 1)
+    b = irs_b200.IRS(**IRS_SMALL, is_double=True, safety_scale=1.3)
+    b.set_stars(stars, rectangular=False, corner=(R, 0.0), theta_star=1.0)
+    b.run()
+    t = _oracle_tree(b)
+    assert t.overflow == 0
+    gi, gg, gn, gs, gd = b.tree_arrays()
+    oi, og, on, os_, od = t.arrays()
+    assert gi.shape[0] > 1.5 * n + 1024  # the first reservation was too small
+    assert b.value("tree_levels") == t.levels
+    np.testing.assert_array_equal(gi, oi)
+    np.testing.assert_array_equal(gg, og)
+    for k in range(gi.shape[0]):
+        assert list(gn[k, :gi[k, 5]]) == list(on[k, :oi[k, 5]])
+        assert list(gs[k, :gi[k, 6]]) == list(os_[k, :oi[k, 6]])
+        assert list(gd[k, :gi[k, 7]]) == list(od[k, :oi[k, 7]])
+    np.testing.assert_array_equal(t.stars(), b.stars.astype(np.float64))
+    assert np.isfinite(b.magnifications).all()
+
+
 def _vertex_positions_oracle(m, t):
     x, y = lattice(m, vertices=True)
     X, Y = np.meshgrid(x, y)
