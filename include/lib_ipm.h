@@ -116,6 +116,9 @@ int get_shoot_ctas_per_sm(IPMHandle* self);
 bool copy_maps_device(IPMHandle* self, void* total, void* minima, void* saddles); /* integer maps to device buffers */
 /* the last run's map (0 total, 1 minima, 2 saddles) into dst[num_pixels_y2][num_pixels_y1], several host threads */
 bool copy_pixels(IPMHandle* self, int which, IPM_DTYPE* dst);
+/* host buffer [num_pixels_y2][num_pixels_y1] that the next run() also fills with its map, copied chunk by
+   chunk while the transfer goes on; one run, NULL to cancel */
+void set_pixels_out(IPMHandle* self, IPM_DTYPE* dst);
 bool derive(IPMHandle* self);                          /* validate + derived parameters, no GPU work */
 double get_value(IPMHandle* self, const char* name);   /* derived / run-time value by name, NaN if unknown */
 /* diagnostics: copies of internal device state */

@@ -108,6 +108,9 @@ int get_shoot_ctas_per_sm(IRSHandle* self);
 bool copy_maps_device(IRSHandle* self, void* total, void* minima, void* saddles); /* integer maps to device buffers */
 /* the last run's map (0 total, 1 minima, 2 saddles) into dst[num_pixels_y2][num_pixels_y1], several host threads */
 bool copy_pixels(IRSHandle* self, int which, int* dst);
+/* host buffer [num_pixels_y2][num_pixels_y1] that the next run() also fills with its map, copied chunk by
+   chunk while the transfer goes on; one run, NULL to cancel */
+void set_pixels_out(IRSHandle* self, int* dst);
 bool derive(IRSHandle* self);
 double get_value(IRSHandle* self, const char* name);
 int get_tree_num_nodes(IRSHandle* self);

@@ -133,6 +133,8 @@ def _bind(lib, kind: str, is_double: bool):
     lib.rerun.restype = C.c_bool
     lib.copy_pixels.argtypes = [vp, C.c_int, C.POINTER(PixT)]
     lib.copy_pixels.restype = C.c_bool
+    lib.set_pixels_out.argtypes = [vp, C.POINTER(PixT)]
+    lib.set_pixels_out.restype = None
     lib.set_band.argtypes = [vp, C.c_longlong, C.c_longlong]
     lib.set_band.restype = None
     lib.set_shoot_launch.argtypes = [vp, C.c_int, C.c_int]

@@ -80,6 +80,7 @@ Pix* get_pixels(Obj* self) { return self->pixels(); }
 Pix* get_pixels_minima(Obj* self) { return self->pixels_minima(); }
 Pix* get_pixels_saddles(Obj* self) { return self->pixels_saddles(); }
 bool copy_pixels(Obj* self, int which, Pix* dst) { return self->copy_pixels(which, dst); }
+void set_pixels_out(Obj* self, Pix* dst) { self->set_pixels_out(dst); }
 #if IRSB_IRS
 double get_t_shoot_rays(Obj* self) { return self->t_shoot; }
 unsigned long long get_num_rays_shot(Obj* self) { return self->num_rays_shot; }

@@ -148,6 +148,8 @@ class MapMaker {
     if (ev_lat0_) cudaEventDestroy(ev_lat0_);
     if (ev_lat1_) cudaEventDestroy(ev_lat1_);
     if (ev_dep1_) cudaEventDestroy(ev_dep1_);
+    for (cudaEvent_t e : out_ev_)
+      if (e) cudaEventDestroy(e);
   }
 
   bool use_fp32() const {
@@ -157,6 +159,10 @@ class MapMaker {
   }
 
   Pix* pixels() { return h_pix.p; }
+  // host buffer of num_pixels_y2 x num_pixels_y1 values that the next run()
+  // also fills with its total map (chunk by chunk, overlapped with the
+  // transfer); applies to one run
+  void set_pixels_out(Pix* dst) { out_user_ = dst; }
   // The map of the last run (0 total, 1 minima, 2 saddles) copied into dst
   // (npix values) by the OpenMP threads (a persistent pool: no thread start
   // per call); false if that map does not exist.
@@ -486,6 +492,9 @@ class MapMaker {
   HistSlot hist_slots_[kMaxHists];
   int n_hist_ = 0;
   cudaEvent_t ev_lat0_ = nullptr, ev_lat1_ = nullptr, ev_dep1_ = nullptr;
+  static constexpr int kOutChunks = 16;
+  cudaEvent_t out_ev_[kOutChunks] = {};
+  Pix* out_user_ = nullptr;  // the next run's map is also copied here (host memory)
   DevVec<StarRec<T>> d_stars_;
   TreeDev<T> tree_;
   FmmDev fmm_;
@@ -508,6 +517,7 @@ class MapMaker {
     IRSB_CKR(cudaEventCreate(&ev_lat0_));
     IRSB_CKR(cudaEventCreate(&ev_lat1_));
     IRSB_CKR(cudaEventCreate(&ev_dep1_));
+    for (cudaEvent_t& e : out_ev_) IRSB_CKR(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     return true;
   }
 
@@ -866,7 +876,31 @@ class MapMaker {
     }
     // maps to the host
     if (!h_pix.alloc(npix)) return false;
-    IRSB_CKR(cudaMemcpyAsync(h_pix.p, dmap, npix * sizeof(Pix), cudaMemcpyDeviceToHost, stream_));
+    Pix* user = out_user_;
+    out_user_ = nullptr;
+    if (user) {
+      // the total map in chunks; the host threads copy each chunk on to the
+      // caller's buffer while the next ones are still in transfer
+      const long long chunk = std::max<long long>(1 << 19, (npix + kOutChunks - 1) / kOutChunks);
+      const int nch = int((npix + chunk - 1) / chunk);
+      for (int i = 0; i < nch; i++) {
+        const long long a = i * chunk, n = std::min(npix, a + chunk) - a;
+        IRSB_CKR(cudaMemcpyAsync(h_pix.p + a, dmap + a, n * sizeof(Pix), cudaMemcpyDeviceToHost, stream_));
+        IRSB_CKR(cudaEventRecord(out_ev_[i], stream_));
+      }
+      for (int i = 0; i < nch; i++) {
+        const long long a = i * chunk, n = std::min(npix, a + chunk) - a;
+        IRSB_CKR(cudaEventSynchronize(out_ev_[i]));
+        const long long sub = (n + 7) / 8;
+#pragma omp parallel for schedule(static) num_threads(8)
+        for (int t = 0; t < 8; t++) {
+          const long long b = a + t * sub, e = std::min(a + n, b + sub);
+          if (b < e) std::memcpy(user + b, h_pix.p + b, size_t(e - b) * sizeof(Pix));
+        }
+      }
+    } else {
+      IRSB_CKR(cudaMemcpyAsync(h_pix.p, dmap, npix * sizeof(Pix), cudaMemcpyDeviceToHost, stream_));
+    }
     if (par) {
       if (!h_pmin.alloc(npix) || !h_psad.alloc(npix)) return false;
       IRSB_CKR(cudaMemcpyAsync(h_pmin.p, dmin, npix * sizeof(Pix), cudaMemcpyDeviceToHost, stream_));

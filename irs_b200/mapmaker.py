@@ -477,9 +477,16 @@ class _MapMaker:
         return out
 
     def run(self):
-        if not self.lib.run(self.obj, self.verbose):
+        # the map lands in a fresh numpy array during run(), chunk by chunk as
+        # it arrives from the device
+        pix_t = self.lib.get_pixels.restype._type_
+        out = np.empty((self.num_pixels_y2, self.num_pixels_y1), dtype=pix_t)
+        self.lib.set_pixels_out(self.obj, out.ctypes.data_as(C.POINTER(pix_t)))
+        ok = self.lib.run(self.obj, self.verbose)
+        self.lib.set_pixels_out(self.obj, None)
+        if not ok:
             raise Exception(f"Error running {self._label}")
-        self.magnifications = self._map(0)
+        self.magnifications = out
         if self.write_parities:
             self.magnifications_minima = self._map(1)
             self.magnifications_saddles = self._map(2)
