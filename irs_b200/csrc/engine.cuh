@@ -150,6 +150,8 @@ class MapMaker {
     if (ev_dep1_) cudaEventDestroy(ev_dep1_);
     for (cudaEvent_t e : out_ev_)
       if (e) cudaEventDestroy(e);
+    if (ev_map_) cudaEventDestroy(ev_map_);
+    if (copy_stream_) cudaStreamDestroy(copy_stream_);
   }
 
   bool use_fp32() const {
@@ -495,6 +497,10 @@ class MapMaker {
   static constexpr int kOutChunks = 16;
   cudaEvent_t out_ev_[kOutChunks] = {};
   Pix* out_user_ = nullptr;  // the next run's map is also copied here (host memory)
+  long long out_chunk_ = 0;
+  int out_nch_ = 0;
+  cudaStream_t copy_stream_ = nullptr;  // the map's transfer beside the histograms
+  cudaEvent_t ev_map_ = nullptr;
   DevVec<StarRec<T>> d_stars_;
   TreeDev<T> tree_;
   FmmDev fmm_;
@@ -518,6 +524,8 @@ class MapMaker {
     IRSB_CKR(cudaEventCreate(&ev_lat1_));
     IRSB_CKR(cudaEventCreate(&ev_dep1_));
     for (cudaEvent_t& e : out_ev_) IRSB_CKR(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    IRSB_CKR(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+    IRSB_CKR(cudaEventCreateWithFlags(&ev_map_, cudaEventDisableTiming));
     return true;
   }
 
@@ -797,6 +805,7 @@ class MapMaker {
     const Pix* dmap = IS_IRS ? (const Pix*)d_pix_.p : (const Pix*)d_map_.p;
     const Pix* dmin = IS_IRS ? (const Pix*)d_pmin_.p : (const Pix*)d_map_min_.p;
     const Pix* dsad = IS_IRS ? (const Pix*)d_psad_.p : (const Pix*)d_map_sad_.p;
+    bool copy_started = false;
     if (IS_IRS) {
       if (!d_red_.alloc_exact(1)) return false;
       IRSB_CKR(cudaMemsetAsync(d_red_.p, 0, sizeof(unsigned long long), stream_));
@@ -843,6 +852,12 @@ class MapMaker {
         std::cerr << "Error. Histogram range is not valid.\n";
         return false;
       }
+      // the map's range is read: its transfer can run beside the histograms
+      // (with parity maps, their range reads would queue behind it)
+      if (!par) {
+        if (!start_map_copy(dmap, npix, copy_stream_)) return false;
+        copy_started = true;
+      }
       if (!make_hist<Pix>(dmap, npix, hist_min, hist_len, factor, 0, hist)) return false;
       if (par) {
         if (!make_hist<Pix>(dmin, npix, hist_min, hist_len, factor, 0, hist_minima)) return false;
@@ -874,39 +889,51 @@ class MapMaker {
         }
       }
     }
-    // maps to the host
-    if (!h_pix.alloc(npix)) return false;
-    Pix* user = out_user_;
-    out_user_ = nullptr;
-    if (user) {
-      // the total map in chunks; the host threads copy each chunk on to the
-      // caller's buffer while the next ones are still in transfer
-      const long long chunk = std::max<long long>(1 << 19, (npix + kOutChunks - 1) / kOutChunks);
-      const int nch = int((npix + chunk - 1) / chunk);
-      for (int i = 0; i < nch; i++) {
-        const long long a = i * chunk, n = std::min(npix, a + chunk) - a;
-        IRSB_CKR(cudaMemcpyAsync(h_pix.p + a, dmap + a, n * sizeof(Pix), cudaMemcpyDeviceToHost, stream_));
-        IRSB_CKR(cudaEventRecord(out_ev_[i], stream_));
-      }
-      for (int i = 0; i < nch; i++) {
-        const long long a = i * chunk, n = std::min(npix, a + chunk) - a;
-        IRSB_CKR(cudaEventSynchronize(out_ev_[i]));
-        const long long sub = (n + 7) / 8;
-#pragma omp parallel for schedule(static) num_threads(8)
-        for (int t = 0; t < 8; t++) {
-          const long long b = a + t * sub, e = std::min(a + n, b + sub);
-          if (b < e) std::memcpy(user + b, h_pix.p + b, size_t(e - b) * sizeof(Pix));
-        }
-      }
-    } else {
-      IRSB_CKR(cudaMemcpyAsync(h_pix.p, dmap, npix * sizeof(Pix), cudaMemcpyDeviceToHost, stream_));
-    }
+    // maps to the host (the total map's transfer may have started above)
+    if (!copy_started && !start_map_copy(dmap, npix, stream_)) return false;
     if (par) {
       if (!h_pmin.alloc(npix) || !h_psad.alloc(npix)) return false;
       IRSB_CKR(cudaMemcpyAsync(h_pmin.p, dmin, npix * sizeof(Pix), cudaMemcpyDeviceToHost, stream_));
       IRSB_CKR(cudaMemcpyAsync(h_psad.p, dsad, npix * sizeof(Pix), cudaMemcpyDeviceToHost, stream_));
     }
     (void)verbose;
+    return finish_map_copy(npix);
+  }
+
+  // The total map to pinned host memory in chunks on stream st (after the map
+  // is final on stream_), an event per chunk.
+  bool start_map_copy(const Pix* dmap, long long npix, cudaStream_t st) {
+    if (!h_pix.alloc(npix)) return false;
+    if (st != stream_) {
+      IRSB_CKR(cudaEventRecord(ev_map_, stream_));
+      IRSB_CKR(cudaStreamWaitEvent(st, ev_map_, 0));
+    }
+    out_chunk_ = std::max<long long>(1 << 19, (npix + kOutChunks - 1) / kOutChunks);
+    out_nch_ = int((npix + out_chunk_ - 1) / out_chunk_);
+    for (int i = 0; i < out_nch_; i++) {
+      const long long a = i * out_chunk_, n = std::min(npix, a + out_chunk_) - a;
+      IRSB_CKR(cudaMemcpyAsync(h_pix.p + a, dmap + a, n * sizeof(Pix), cudaMemcpyDeviceToHost, st));
+      IRSB_CKR(cudaEventRecord(out_ev_[i], st));
+    }
+    return true;
+  }
+  // Waits for the chunks; with a caller buffer set (set_pixels_out), the host
+  // threads copy each chunk on while the next ones are still in transfer.
+  bool finish_map_copy(long long npix) {
+    Pix* user = out_user_;
+    out_user_ = nullptr;
+    for (int i = 0; i < out_nch_; i++) {
+      const long long a = i * out_chunk_, n = std::min(npix, a + out_chunk_) - a;
+      IRSB_CKR(cudaEventSynchronize(out_ev_[i]));
+      if (!user) continue;
+      const long long sub = (n + 7) / 8;
+#pragma omp parallel for schedule(static) num_threads(8)
+      for (int t = 0; t < 8; t++) {
+        const long long b = a + t * sub, e = std::min(a + n, b + sub);
+        if (b < e) std::memcpy(user + b, h_pix.p + b, size_t(e - b) * sizeof(Pix));
+      }
+    }
+    out_nch_ = 0;
     return true;
   }
 
