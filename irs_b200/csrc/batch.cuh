@@ -639,9 +639,7 @@ class BatchMaker {
     }
     const DepositMaps mt{d_acc_.p, d_diff_.p};
     const int gr = std::max(1, std::min(ceil_div((long long)npy_ * R * 32, 256), 148 * 8));
-    ipm_resolve_rows<<<gr, 256, 0, s>>>(npx_, npy_ * R, mt);
-    const int g2 = int(std::max<long long>(1, std::min<long long>((npix * R + 255) / 256, 148LL * 16)));
-    ipm_finalize<T><<<g2, 256, 0, s>>>(npix * R, d_acc_.p, nullptr, nullptr, d_out_.p, nullptr, nullptr, 0);
+    ipm_resolve_rows_out<T><<<gr, 256, 0, s>>>(npx_, npy_ * R, mt, d_out_.p);  // resolve and convert
     IRSB_LAUNCH_CK("batch maps");
     return true;
   }

@@ -681,16 +681,18 @@ class MapMaker {
         if (par) {
           ipm_resolve_rows<<<gr, 256, 0, stream_>>>(p.num_pixels_y.re, p.num_pixels_y.im, mmin);
           ipm_resolve_rows<<<gr, 256, 0, stream_>>>(p.num_pixels_y.re, p.num_pixels_y.im, msad);
-        } else {
-          ipm_resolve_rows<<<gr, 256, 0, stream_>>>(p.num_pixels_y.re, p.num_pixels_y.im, mt);
+        } else {  // resolve and convert in one pass
+          ipm_resolve_rows_out<T><<<gr, 256, 0, stream_>>>(p.num_pixels_y.re, p.num_pixels_y.im, mt, d_map_.p);
         }
         IRSB_LAUNCH_CK("ipm_resolve_rows");
       }
-      launches += par ? 4 : 3;
-      int g2 = int(std::max<long long>(1, std::min<long long>((npix + 255) / 256, 148LL * 16)));
-      ipm_finalize<T><<<g2, 256, 0, stream_>>>(npix, d_acc_.p, d_acc_min_.p, d_acc_sad_.p, d_map_.p, d_map_min_.p,
-                                                 d_map_sad_.p, par ? 1 : 0);
-      IRSB_LAUNCH_CK("ipm_finalize");
+      launches += par ? 4 : 2;
+      if (par) {
+        int g2 = int(std::max<long long>(1, std::min<long long>((npix + 255) / 256, 148LL * 16)));
+        ipm_finalize<T><<<g2, 256, 0, stream_>>>(npix, d_acc_.p, d_acc_min_.p, d_acc_sad_.p, d_map_.p,
+                                                   d_map_min_.p, d_map_sad_.p, 1);
+        IRSB_LAUNCH_CK("ipm_finalize");
+      }
     }
     return true;
   }
