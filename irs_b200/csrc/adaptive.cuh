@@ -115,10 +115,9 @@ __device__ __forceinline__ double2 eval_point_f32(const ShootParams& sp, const L
   float Ar = 0.f, Ai = 0.f;
   for (int k = sp.p - 1; k >= 0; k--) {
     const float2 c = coef[k];
-    const float tr = fmaf(Ar, dzr, -Ai * dzi);
-    const float tt = fmaf(Ar, dzi, Ai * dzr);
-    Ar = tr + c.x;
-    Ai = tt + c.y;
+    const float ar = fmaf(Ar, dzr, fmaf(-Ai, dzi, c.x));  // as shoot_f32
+    Ai = fmaf(Ar, dzi, fmaf(Ai, dzr, c.y));
+    Ar = ar;
   }
   const float Sx = sx + cxr, Sy = sy + cyr;
   const float wr = fmaf(float(lin_x), ux, -(Sx + Ar));

@@ -355,10 +355,10 @@ __device__ __forceinline__ void shoot_f32_tile(const ShootParams& sp, const Leaf
             Dr[r] = fmaf(c.x, float(k), tr);
             Di[r] = fmaf(c.y, float(k), tt);
           }
-          float tr = fmaf(Ar[r], dzr[r], -Ai[r] * dzi[r]);
-          float tt = fmaf(Ar[r], dzi[r], Ai[r] * dzr[r]);
-          Ar[r] = tr + c.x;
-          Ai[r] = tt + c.y;
+          // A <- A dz + c as two FMA chains (4 operations per order)
+          const float ar = fmaf(Ar[r], dzr[r], fmaf(-Ai[r], dzi[r], c.x));
+          Ai[r] = fmaf(Ar[r], dzi[r], fmaf(Ai[r], dzr[r], c.y));
+          Ar[r] = ar;
         }
       }
       // ---- output
