@@ -92,9 +92,9 @@ __device__ __forceinline__ double2 eval_point_f32(const ShootParams& sp, const L
   const int nn = L.nn;
   const float4* near = L.near;
   float sx = 0.f, sy = 0.f, cxr = 0.f, cyr = 0.f;
-  for (int s0 = 0; s0 < nn; s0 += 8) {
+  for (int s0 = 0; s0 < nn; s0 += 16) {
     float bx = 0.f, by = 0.f;
-    for (int s = s0; s < s0 + 8 && s < nn; s++) {
+    for (int s = s0; s < s0 + 16 && s < nn; s++) {
       const float4 st = near[s];
       const float ex = ux - st.x, ey = uy - st.y;
       const float r2 = fmaf(ey, ey, ex * ex);

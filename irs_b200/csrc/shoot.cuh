@@ -13,7 +13,7 @@
 //     array_functions.cuh:70-75).
 //   * shoot_f32 -- the FP32 form. Coordinates are taken relative to the leaf
 //     centre; the near-field sum runs in FP32 with blocked two-sum
-//     compensation (naive partial sums of 8 stars folded into a compensated
+//     compensation (naive partial sums of 16 stars folded into a compensated
 //     accumulator); the far field is an FP32 Horner evaluation of coefficients
 //     built in FP64; the linear part of the lens equation is applied at the
 //     leaf centre in FP64 and the final cell-local -> global pixel conversion
@@ -295,9 +295,10 @@ __device__ __forceinline__ void shoot_f32_tile(const ShootParams& sp, const Leaf
       float dxx[R], dxy[R];  // derivative sums (parity only)
 #pragma unroll
       for (int r = 0; r < R; r++) sx[r] = sy[r] = cxr[r] = cyr[r] = dxx[r] = dxy[r] = 0.f;
-      // blocks of 8 stars (the last one of 4 when nn4 is not a multiple of
-      // 8), each block's sum added to the running sum by a two-sum; a
-      // thread's points share ux, so ex and ex^2 are formed once per star
+      // blocks of 16 stars (the last one of 4, 8 or 12 when nn4 is not a
+      // multiple of 16), each block's sum added to the running sum by a
+      // two-sum; a thread's points share ux, so ex and ex^2 are formed once
+      // per star
       auto star = [&](const float4 st, float* bx, float* by) {
         const float ex = ux - st.x, ex2 = ex * ex;
 #pragma unroll
@@ -315,15 +316,18 @@ __device__ __forceinline__ void shoot_f32_tile(const ShootParams& sp, const Leaf
           }
         }
       };
-      for (int s0 = 0; s0 < nn4; s0 += 8) {
+      for (int s0 = 0; s0 < nn4; s0 += 16) {
         float bx[R], by[R];
 #pragma unroll
         for (int r = 0; r < R; r++) bx[r] = by[r] = 0.f;
 #pragma unroll
         for (int s = 0; s < 4; s++) star(s_near[s0 + s], bx, by);
-        if (s0 + 8 <= nn4) {
 #pragma unroll
-          for (int s = 4; s < 8; s++) star(s_near[s0 + s], bx, by);
+        for (int g = 1; g < 4; g++) {
+          if (s0 + 4 * (g + 1) <= nn4) {
+#pragma unroll
+            for (int s = 0; s < 4; s++) star(s_near[s0 + 4 * g + s], bx, by);
+          }
         }
 #pragma unroll
         for (int r = 0; r < R; r++) {  // two-sum of the block into the running sum
