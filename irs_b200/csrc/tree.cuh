@@ -143,39 +143,6 @@ __global__ void tree_near_count(int beg, int end, LevelRange lr, const int* __re
   if ((threadIdx.x & 31) == 0) atomicMax(&dstat[0], local_max);
 }
 
-// The 4 children of split node k at c0 .. c0 + 3 (make_child,
-// tree_node.cuh:151-168), with their descent boxes.
-template <typename T>
-__device__ __forceinline__ void node_children(int k, int c0, T* cx, T* cy, T* hl, int* level, int* parent,
-                                              int* child0, int* sbeg, int* scnt, int* rid, int* n_nbr, int* n_sil,
-                                              int* n_dil, double* lox, double* hix, double* loy, double* hiy) {
-  child0[k] = c0;
-  T h = hl[k] / 2;
-  T pcx = cx[k], pcy = cy[k];
-  const T ox[4] = {T(1), T(-1), T(-1), T(1)};
-  const T oy[4] = {T(1), T(1), T(-1), T(-1)};
-  double plox = lox[k], phix = hix[k], ploy = loy[k], phiy = hiy[k];
-  for (int q = 0; q < 4; q++) {
-    int c = c0 + q;
-    cx[c] = pcx + h * ox[q];
-    cy[c] = pcy + h * oy[q];
-    hl[c] = h;
-    level[c] = level[k] + 1;
-    parent[c] = k;
-    rid[c] = rid[k];
-    child0[c] = -1;
-    sbeg[c] = sbeg[k];
-    scnt[c] = 0;
-    n_nbr[c] = n_sil[c] = n_dil[c] = 0;
-    // x >= pcx for q = 0, 3; y >= pcy for q = 0, 1
-    bool right = (q == 0 || q == 3), top = (q == 0 || q == 1);
-    lox[c] = right ? double(pcx) : plox;
-    hix[c] = right ? phix : double(pcx);
-    loy[c] = top ? double(pcy) : ploy;
-    hiy[c] = top ? phiy : double(pcy);
-  }
-}
-
 template <typename T>
 __global__ void tree_make_children(int beg, int end, int child_base, LevelRange lr, const int* __restrict__ stop,
                                    const int* __restrict__ split, const long long* __restrict__ rank, T* cx, T* cy,
@@ -192,86 +159,32 @@ __global__ void tree_make_children(int beg, int end, int child_base, LevelRange 
       child0[k] = -1;
       continue;
     }
-    node_children<T>(k, child_base + 4 * int(rank[k - beg]), cx, cy, hl, level, parent, child0, sbeg, scnt, rid, n_nbr,
-                     n_sil, n_dil, lox, hix, loy, hiy);
-  }
-}
-
-// One level in one block of 1024 threads, for levels of at most a few
-// thousand nodes: the split flags (tree_near_count), their exclusive scan,
-// the next level's extent (tree_advance_level) and the children
-// (tree_make_children) in one launch instead of six. Each thread takes a
-// contiguous run of the level's nodes, so the ranks are those of the scan.
-template <typename T>
-__global__ void __launch_bounds__(1024) tree_level_step(
-    int l, int nlev, int* off, int* lvl_n, int node_cap, int* stop, int* dstat, const int* __restrict__ nbr,
-    int* split, long long* rank, T* cx, T* cy, T* hl, int* level, int* parent, int* child0, int* sbeg, int* scnt,
-    int* rid, int* n_nbr, int* n_sil, int* n_dil, double* lox, double* hix, double* loy, double* hiy) {
-  __shared__ int s_warp[32];
-  __shared__ int s_halt;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int beg = off[l], end = off[l + 1], n = end - beg;
-  const int per = (n + int(blockDim.x) - 1) / int(blockDim.x);
-  const int a = beg + int(threadIdx.x) * per, b = min(end, a + per);
-  int cnt = 0, mx = 0;
-  for (int k = a; k < b; k++) {
-    int c = scnt[k];
-    const int nn = n_nbr[k];
-    for (int j = 0; j < nn; j++) c += scnt[nbr[k * kMaxNeighbors + j]];
-    const int sp = c > kMaxStarsDirect ? 1 : 0;
-    split[k - beg] = sp;
-    cnt += sp;
-    mx = max(mx, c);
-  }
-  mx = __reduce_max_sync(0xffffffffu, mx);
-  if (lane == 0 && mx > 0) atomicMax(&dstat[0], mx);
-  // exclusive scan of the per-thread counts
-  int incl = cnt;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int u = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += u;
-  }
-  if (lane == 31) s_warp[w] = incl;
-  __syncthreads();
-  if (w == 0) {
-    const int nw = int(blockDim.x) >> 5;
-    int v = lane < nw ? s_warp[lane] : 0, vi = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int u = __shfl_up_sync(0xffffffffu, vi, o);
-      if (lane >= o) vi += u;
+    int c0 = child_base + 4 * int(rank[k - beg]);
+    child0[k] = c0;
+    T h = hl[k] / 2;
+    T pcx = cx[k], pcy = cy[k];
+    const T ox[4] = {T(1), T(-1), T(-1), T(1)};
+    const T oy[4] = {T(1), T(1), T(-1), T(-1)};
+    double plox = lox[k], phix = hix[k], ploy = loy[k], phiy = hiy[k];
+    for (int q = 0; q < 4; q++) {
+      int c = c0 + q;
+      cx[c] = pcx + h * ox[q];
+      cy[c] = pcy + h * oy[q];
+      hl[c] = h;
+      level[c] = level[k] + 1;
+      parent[c] = k;
+      rid[c] = rid[k];
+      child0[c] = -1;
+      sbeg[c] = sbeg[k];
+      scnt[c] = 0;
+      n_nbr[c] = n_sil[c] = n_dil[c] = 0;
+      // x >= pcx for q = 0, 3; y >= pcy for q = 0, 1
+      bool right = (q == 0 || q == 3), top = (q == 0 || q == 1);
+      lox[c] = right ? double(pcx) : plox;
+      hix[c] = right ? phix : double(pcx);
+      loy[c] = top ? double(pcy) : ploy;
+      hiy[c] = top ? phiy : double(pcy);
     }
-    if (lane < nw) s_warp[lane] = vi - v;  // exclusive over the warps
-    if (lane == 31) {  // the next level's extent, as tree_advance_level
-      long long nsplit = *stop ? 0 : vi;
-      if (nsplit > 0 && l == nlev - 1) {
-        atomicOr(&dstat[1], kErrLevelOverflow);
-        *stop = 1;
-        nsplit = 0;
-      }
-      if (end + 4 * nsplit > node_cap) {
-        atomicOr(&dstat[1], kErrNodeOverflow);
-        *stop = 1;
-        nsplit = 0;
-      }
-      off[l + 2] = end + int(4 * nsplit);
-      lvl_n[l + 1] = int(4 * nsplit);
-      s_halt = *stop;
-    }
-  }
-  __syncthreads();
-  long long r = s_warp[w] + (incl - cnt);
-  const bool halt = s_halt != 0;
-  for (int k = a; k < b; k++) {
-    if (halt || !split[k - beg]) {
-      child0[k] = -1;
-      continue;
-    }
-    rank[k - beg] = r;
-    node_children<T>(k, end + 4 * int(r), cx, cy, hl, level, parent, child0, sbeg, scnt, rid, n_nbr, n_sil, n_dil,
-                     lox, hix, loy, hiy);
-    r++;
   }
 }
 
@@ -724,22 +637,13 @@ bool build_tree(TreeDev<T>& t, StarRec<T>* stars, int nstars, T root_hl, cudaStr
       for (; l < lend; l++) {
         const LevelRange lr{t.d_off.p, l}, next{t.d_off.p, l + 1};
         const int g1 = grid(l, 256);
-        if (l <= 6) {  // at most 4096 nodes: one block does the level's bookkeeping
-          tree_level_step<T><<<1, 1024, 0, s>>>(l, kMaxLevels, t.d_off.p, t.d_lvl_n.p, int(cap), t.d_stop.p, t.dstat.p,
-                                                t.nbr.p, t.split.p, t.rank.p, t.cx.p, t.cy.p, t.hl.p, t.level.p,
-                                                t.parent.p, t.child0.p, t.sbeg.p, t.scnt.p, t.rid.p, t.n_nbr.p,
-                                                t.n_sil.p, t.n_dil.p, t.lox.p, t.hix.p, t.loy.p, t.hiy.p);
-          t.launches -= 5;
-        } else {
-          tree_near_count<<<g1, 256, 0, s>>>(0, 0, lr, t.scnt.p, t.nbr.p, t.n_nbr.p, t.split.p, t.dstat.p);
-          if (!exclusive_scan_dev<int>(t.split.p, t.d_lvl_n.p + l, cap, t.rank.p, t.scan, s)) return false;
-          tree_advance_level<<<1, 1, 0, s>>>(l, kMaxLevels, t.d_off.p, t.d_lvl_n.p, t.scan.sum.p, int(cap),
-                                             t.d_stop.p, t.dstat.p);
-          tree_make_children<T><<<g1, 256, 0, s>>>(0, 0, 0, lr, t.d_stop.p, t.split.p, t.rank.p, t.cx.p, t.cy.p,
-                                                   t.hl.p, t.level.p, t.parent.p, t.child0.p, t.sbeg.p, t.scnt.p,
-                                                   t.rid.p, t.n_nbr.p, t.n_sil.p, t.n_dil.p, t.lox.p, t.hix.p,
-                                                   t.loy.p, t.hiy.p);
-        }
+        tree_near_count<<<g1, 256, 0, s>>>(0, 0, lr, t.scnt.p, t.nbr.p, t.n_nbr.p, t.split.p, t.dstat.p);
+        if (!exclusive_scan_dev<int>(t.split.p, t.d_lvl_n.p + l, cap, t.rank.p, t.scan, s)) return false;
+        tree_advance_level<<<1, 1, 0, s>>>(l, kMaxLevels, t.d_off.p, t.d_lvl_n.p, t.scan.sum.p, int(cap), t.d_stop.p,
+                                           t.dstat.p);
+        tree_make_children<T><<<g1, 256, 0, s>>>(0, 0, 0, lr, t.d_stop.p, t.split.p, t.rank.p, t.cx.p, t.cy.p, t.hl.p,
+                                                 t.level.p, t.parent.p, t.child0.p, t.sbeg.p, t.scnt.p, t.rid.p,
+                                                 t.n_nbr.p, t.n_sil.p, t.n_dil.p, t.lox.p, t.hix.p, t.loy.p, t.hiy.p);
         if (l == 0) {  // the root: every star, on many blocks
           if (!wide_partition<T, 1>(t, lr, stars, nstars, nchunks, s)) return false;
           t.launches += 3;
