@@ -450,7 +450,7 @@ __global__ void __launch_bounds__(256) ada_window_errors(AdaGeom g, const int* _
       }
       // where the plain map holds less than the tile's own flux, the tile's
       // flux is the reference
-      if (touched && mode >= 1) tot += fmax(double(ref[(long long)y * g.npx + x]), double(a16));
+      if (touched && mode >= 1) tot += fmax(double((long long)ref[(long long)y * g.npx + x]), double(a16));
     }
 #pragma unroll
     for (int c = 0; c < 5; c++) {

@@ -10,20 +10,27 @@
 // factor * |A ∩ pixel| / |A|.
 //
 // How, differently by design:
-//   * the overlap of a triangle with a pixel is computed directly from
-//     Green's theorem instead of by successive polygon clips: the edges are
-//     clipped once per row strip (row_geometry), and each pixel of the row
-//     then only clamps those segments to its column (pixel_coverage):
-//     register-only arithmetic, no polygon arrays;
+//   * no polygon clipping: each triangle's area is spread over the pixels by
+//     accumulating its edges into a per-row difference array (a coverage
+//     accumulation rasterizer). An edge piece lying inside pixel column c of
+//     row strip r, running from height ya to yb, contributes the cover
+//     K = F(ya) - F(yb) to every pixel right of c and the share
+//     K (1 - f) to pixel c itself, f being the piece's mean x inside the
+//     column; in the difference array that is K - a1 at c and a1 = round(K f)
+//     at c + 1, so that the row's prefix sum gives each pixel's covered area.
+//     F(y) = round(y * scale) is evaluated once per break point (a vertex, a
+//     crossing of a row line or of a column line) and shared by the two pieces
+//     meeting there, so the covers of every row of a triangle sum to exactly
+//     zero: nothing leaks right of a triangle, whatever the rounding;
 //   * rows of a triangle are independent work items; a warp expands the rows
 //     of its 64 triangles and shares them out 32 at a time;
-//   * pixels inside both the bottom and the top chord of a row strip are fully
-//     covered (area exactly 1) and are added as a run through a per-row
-//     difference array;
+//   * pieces left of the map are merged into one cover at the map's first
+//     column; pieces right of it are dropped;
 //   * coordinates are relative to an integer origin at the triangle's
-//     lower-left pixel; the map accumulates unsigned 64-bit fixed point (2^32
-//     per unit) with integer atomics, so the result does not depend on thread
-//     order: given the same corner positions the map is bit-exact.
+//     lower-left pixel; the map accumulates 64-bit fixed point (2^32 per unit,
+//     modulo 2^64, read as signed) with integer atomics, so the result does not
+//     depend on thread order: given the same corner positions the map is
+//     bit-exact.
 // Every floating-point operation is an explicitly rounded intrinsic (no FMA
 // contraction), so a host implementation with the same operation sequence
 // reproduces the map bit for bit.
@@ -72,12 +79,14 @@ struct DepositMaps {
 };
 
 // A triangle prepared for deposition: CCW vertices relative to the integer
-// origin (ox, oy), per-edge reciprocals, fixed-point scale and target map.
+// origin (ox, oy), per-edge slopes, the vertices' heights times the
+// fixed-point scale, and the target map.
 template <typename D>
 struct Tri {
   D x[3], y[3];     // CCW, relative to (ox, oy)
-  D idy[3];         // 1 / (y[k+1] - y[k]) (0 for a zero difference)
-  D sl[3];          // slope (y[k+1] - y[k]) * (1 / (x[k+1] - x[k])); 0 for a vertical edge or an overflow
+  D pv[3];          // y[k] * scale (unrounded): F(y[k]) = round(pv[k])
+  D gxy[3];         // dx * (1 / dy) of edge k -> k+1 (0 for a horizontal edge)
+  D gyx[3];         // dy * (1 / dx) of edge k -> k+1 (0 for a vertical edge or an overflow)
   D scale;          // factor * 2^32 / |area|
   int ox, oy;
   int rlo, nrows;   // first row (relative) and number of rows to visit
@@ -105,7 +114,7 @@ __device__ __forceinline__ Tri<D> setup_head(double ax, double ay, double bx, do
   t.map = 0;
   t.single = 0;
   t.scale = D(0);
-  for (int k = 0; k < 3; k++) t.x[k] = t.y[k] = t.sl[k] = t.idy[k] = D(0);
+  for (int k = 0; k < 3; k++) t.x[k] = t.y[k] = t.pv[k] = t.gxy[k] = t.gyx[k] = D(0);
   if (isnan(ax) || isnan(ay) || isnan(bx) || isnan(by) || isnan(cx) || isnan(cy)) return t;
   double fx = floor(fmin(ax, fmin(bx, cx)));
   double fy = floor(fmin(ay, fmin(by, cy)));
@@ -146,8 +155,7 @@ __device__ __forceinline__ Tri<D> setup_head(double ax, double ay, double bx, do
   t.ox = ox;
   t.oy = oy;
   int rlo = 0 > -oy ? 0 : -oy;
-  int rhi = int(floor(mxy));
-  if (rhi > npy - 1 - oy) rhi = npy - 1 - oy;
+  int rhi = mxy < D(npy - oy) ? int(floor(mxy)) : npy - 1 - oy;
   t.rlo = rlo;
   t.nrows = rhi >= rlo ? rhi - rlo + 1 : 0;
   // inside one pixel of the map: all its area goes there
@@ -155,19 +163,20 @@ __device__ __forceinline__ Tri<D> setup_head(double ax, double ay, double bx, do
   return t;
 }
 
-// Edge reciprocals, slopes and the fixed-point scale of a triangle that
+// Slopes, scaled vertex heights and the fixed-point scale of a triangle that
 // deposits row by row (nrows > 0, not single).
 template <typename D>
 __device__ __forceinline__ void setup_tail(Tri<D>& t, D factor) {
+  t.scale = RN<D>::div(RN<D>::mul(factor, D(kFixScale)), t.scale);
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     const int j = k == 2 ? 0 : k + 1;
     const D dx = RN<D>::sub(t.x[j], t.x[k]), dy = RN<D>::sub(t.y[j], t.y[k]);
-    t.idy[k] = rcp_or_zero(dy);
+    t.gxy[k] = RN<D>::mul(dx, rcp_or_zero(dy));
     const D g = RN<D>::mul(dy, rcp_or_zero(dx));
-    t.sl[k] = dabs(g) <= std::numeric_limits<D>::max() ? g : D(0);
+    t.gyx[k] = dabs(g) <= std::numeric_limits<D>::max() ? g : D(0);
+    t.pv[k] = RN<D>::mul(t.y[k], t.scale);
   }
-  t.scale = RN<D>::div(RN<D>::mul(factor, D(kFixScale)), t.scale);
 }
 
 // Shared-memory staging of the 64 triangles of a warp's 32 cells that go row
@@ -206,152 +215,166 @@ struct TriSlots {
 };
 constexpr int kDepositWarps = 8;  // warps per CTA of the deposition kernels (256 threads)
 
-// Geometry of one row strip [rb, rt = rb + 1] of a triangle.
-//   Strip segments: each edge clipped to the strip, endpoints (xa, ya) ->
-//   (xb, yb) with y relative to rb, a zero segment where the edge misses the
-//   strip. A horizontal edge belongs to the strip only on [rb, rt), so an edge
-//   lying on the line between two rows is counted once (by the top chord of
-//   the row below).
-//   Chords: x-extent of the triangle on the lines y = rb and y = rt (an edge
-//   reaching the line contributes its crossing, x1 + ((y - y1) / dy) dx, or
-//   both ends when it lies on the line).
-template <typename D>
-struct Strip {
-  D xa[3], ya[3], xb[3], yb[3];
+// Difference-array adds of one row, merged while consecutive adds hit the
+// same column (the shared column of two neighbouring pieces of an edge).
+// Columns are relative to the triangle's origin; those at or right of the
+// map's last column + 1 (chi) are dropped.
+struct RowAdds {
+  unsigned long long* drow;  // difference-array row at relative column 0
+  int chi;
+  int idx = -(1 << 30);
+  unsigned long long val = 0;
+  __device__ __forceinline__ void flush() {
+    if (idx < chi && val) atomicAdd(drow + idx, val);
+  }
+  __device__ __forceinline__ void add(int c, unsigned long long v) {
+    if (c != idx) {
+      flush();
+      idx = c;
+      val = v;
+    } else {
+      val += v;
+    }
+  }
 };
 
+// Edge (xk, yk) -> (xj, yj) of a triangle inside row strip [rb, rt = rb + 1]
+// (relative): the pieces between its entry and exit points, split at the
+// column lines, into the row's difference array. pvk, pvj: the vertices'
+// heights times the scale; g = dx/dy, h = dy/dx of the edge; pb, pt: rb and
+// rt times the scale. Columns left of the map (relative column clo) are
+// merged into one cover at clo; the part right of column chi is dropped.
 template <typename D>
-__device__ __forceinline__ void extend(bool& any, D& lo, D& hi, D a, D b) {
-  const D mn = a < b ? a : b, mx = a > b ? a : b;
-  lo = any ? (mn < lo ? mn : lo) : mn;
-  hi = any ? (mx > hi ? mx : hi) : mx;
-  any = true;
-}
-
-// Fills the strip segments and both chords; returns false when the triangle
-// does not enter the strip, else sets its x-extent [xlo, xhi] there.
-template <typename D>
-__device__ __forceinline__ bool row_geometry(const Tri<D>& t, D rb, D rt, Strip<D>& g, D& xlo, D& xhi, bool& hb,
-                                             D& cb0, D& cb1, bool& ht, D& ct0, D& ct1) {
-  bool any = false;
-  xlo = xhi = cb0 = cb1 = ct0 = ct1 = D(0);
-  hb = ht = false;
-#pragma unroll
-  for (int k = 0; k < 3; k++) {
-    const int j = k == 2 ? 0 : k + 1;
-    const D x1 = t.x[k], y1 = t.y[k], x2 = t.x[j], y2 = t.y[j];
-    const D dx = RN<D>::sub(x2, x1), dy = RN<D>::sub(y2, y1);
-    const bool on_b = (y1 <= rb && rb <= y2) || (y2 <= rb && rb <= y1);
-    const bool on_t = (y1 <= rt && rt <= y2) || (y2 <= rt && rt <= y1);
-    D t0 = D(0), t1 = D(1);
-    bool ok;
-    if (dy != D(0)) {
-      const D ta = RN<D>::mul(RN<D>::sub(rb, y1), t.idy[k]), tb = RN<D>::mul(RN<D>::sub(rt, y1), t.idy[k]);
-      if (on_b) {
-        const D p = RN<D>::add(x1, RN<D>::mul(ta, dx));
-        extend(hb, cb0, cb1, p, p);
-      }
-      if (on_t) {
-        const D p = RN<D>::add(x1, RN<D>::mul(tb, dx));
-        extend(ht, ct0, ct1, p, p);
-      }
-      const D lo = ta < tb ? ta : tb, hi = ta > tb ? ta : tb;
-      t0 = lo > t0 ? lo : t0;
-      t1 = hi < t1 ? hi : t1;
-      ok = t0 < t1;
+__device__ __forceinline__ void deposit_edge_row(D xk, D yk, D xj, D yj, D pvk, D pvj, D g, D h, D scale, D rb,
+                                                 D rt, D pb, D pt, int clo, int chi, RowAdds& out) {
+  if (yk == yj) return;  // a horizontal edge has no cover
+  const D ylo = yk < yj ? yk : yj, yhi = yk > yj ? yk : yj;
+  if (!(ylo < rt && yhi > rb)) return;
+  const D xlo = xk < xj ? xk : xj, xhi = xk > xj ? xk : xj;
+  // entry (a) and exit (b) of the edge in the strip, in the edge's direction:
+  // a vertex, or the crossing with a row line (x from the edge, y exact)
+  D xa, ya, qa, xb, yb, qb;
+  const bool up = yj > yk;
+  const D ea = up ? rb : rt, eb = up ? rt : rb;  // row lines where the edge enters / leaves
+  const D pea = up ? pb : pt, peb = up ? pt : pb;
+  if (up ? (yk >= rb) : (yk <= rt)) {
+    xa = xk, ya = yk, qa = pvk;
+  } else {
+    const D x = RN<D>::add(xk, RN<D>::mul(RN<D>::sub(ea, yk), g));
+    xa = x < xlo ? xlo : (x > xhi ? xhi : x), ya = ea, qa = pea;
+  }
+  if (up ? (yj <= rt) : (yj >= rb)) {
+    xb = xj, yb = yj, qb = pvj;
+  } else {
+    const D x = RN<D>::add(xk, RN<D>::mul(RN<D>::sub(eb, yk), g));
+    xb = x < xlo ? xlo : (x > xhi ? xhi : x), yb = eb, qb = peb;
+  }
+  const D plo = ya < yb ? ya : yb, phi = ya > yb ? ya : yb;
+  // height (times scale) where the edge crosses the column line X, kept inside the piece's range
+  auto cross = [&](D X) {
+    D y = RN<D>::add(yk, RN<D>::mul(RN<D>::sub(X, xk), h));
+    y = y < plo ? plo : (y > phi ? phi : y);
+    return RN<D>::mul(y, scale);
+  };
+  // columns visited: right- or leftward from the entry's column to the exit's
+  // (positions beyond the map are clamped first: only their side matters)
+  const D cl = D(clo - 1), ch = D(chi + 1);
+  const D ua = xa < cl ? cl : (xa > ch ? ch : xa), ub = xb < cl ? cl : (xb > ch ? ch : xb);
+  int dir, c, ce;
+  if (xb > xa) {
+    dir = 1, c = int(floor(ua)), ce = int(ceil(ub)) - 1;
+  } else if (xb < xa) {
+    dir = -1, c = int(ceil(ua)) - 1, ce = int(floor(ub));
+  } else {
+    dir = 0, c = ce = int(floor(ua));
+  }
+  long long fa = (long long)RN<D>::to_fix(qa);
+  long long fb = (long long)RN<D>::to_fix(qb);
+  if (dir >= 0) {
+    if (ce < clo) {  // all of it left of the map
+      out.add(clo, (unsigned long long)(fa - fb));
+      return;
+    }
+    if (c >= chi) return;
+    if (c < clo) {  // the part left of the map: one cover at its first column
+      const D X = D(clo);
+      const D q = cross(X);
+      const long long f = (long long)RN<D>::to_fix(q);
+      out.add(clo, (unsigned long long)(fa - f));
+      xa = X, qa = q, fa = f, c = clo;
+    }
+    if (ce >= chi) {  // stop at the map's right edge
+      const D X = D(chi);
+      xb = X, qb = cross(X), fb = (long long)RN<D>::to_fix(qb), ce = chi - 1;
+    }
+  } else {
+    if (c < clo) {
+      out.add(clo, (unsigned long long)(fa - fb));
+      return;
+    }
+    if (ce >= chi) return;
+    if (c >= chi) {  // start at the map's right edge
+      const D X = D(chi);
+      xa = X, qa = cross(X), fa = (long long)RN<D>::to_fix(qa), c = chi - 1;
+    }
+  }
+  const bool left_tail = dir < 0 && ce < clo;  // leftward past the map's first column
+  const int cstop = left_tail ? clo : ce;
+  for (;;) {
+    const bool last = c == cstop;
+    D xq, qq;
+    long long fq;
+    if (!last || left_tail) {
+      xq = D(dir > 0 ? c + 1 : c);  // the column line where the piece leaves column c
+      qq = cross(xq);
+      fq = (long long)RN<D>::to_fix(qq);
     } else {
-      if (on_b) extend(hb, cb0, cb1, x1, x2);
-      if (on_t) extend(ht, ct0, ct1, x1, x2);
-      ok = y1 >= rb && y1 < rt;
+      xq = xb, qq = qb, fq = fb;
     }
-    D xa = D(0), ya = D(0), xb = D(0), yb = D(0);
-    if (ok) {
-      xa = RN<D>::add(x1, RN<D>::mul(t0, dx));
-      xb = RN<D>::add(x1, RN<D>::mul(t1, dx));
-      ya = RN<D>::sub(RN<D>::add(y1, RN<D>::mul(t0, dy)), rb);
-      yb = RN<D>::sub(RN<D>::add(y1, RN<D>::mul(t1, dy)), rb);
-      extend(any, xlo, xhi, xa, xb);
+    const long long K = fa - fq;
+    D fm = RN<D>::sub(RN<D>::mul(RN<D>::add(xa, xq), D(0.5)), D(c));
+    fm = fm < D(0) ? D(0) : (fm > D(1) ? D(1) : fm);
+    const long long a1 = (long long)RN<D>::to_fix(RN<D>::mul(RN<D>::sub(qa, qq), fm));
+    const long long a0 = K - a1;
+    if (dir >= 0) {
+      out.add(c, (unsigned long long)a0);
+      out.add(c + 1, (unsigned long long)a1);
+    } else {
+      out.add(c + 1, (unsigned long long)a1);
+      out.add(c, (unsigned long long)a0);
     }
-    g.xa[k] = xa;
-    g.ya[k] = ya;
-    g.xb[k] = xb;
-    g.yb[k] = yb;
+    xa = xq, qa = qq, fa = fq;
+    if (last) break;
+    c += dir;
   }
-  return any;
+  if (left_tail) out.add(clo, (unsigned long long)(fa - fb));
 }
 
-// Area of the triangle inside the pixel [c, c+1] x [rb, rb+1] from Green's
-// theorem, area = -(sum over the boundary of the integral of (y - rb) dx):
-// each strip segment restricted to the column (both ends clamped to
-// [c, c+1], an edge being monotone in x) is a trapezoid; the pixel's top side
-// adds the top chord's length inside the column; the vertical sides and the
-// bottom side add nothing.
-template <typename D>
-__device__ __forceinline__ D pixel_coverage(const Tri<D>& t, const Strip<D>& g, D c, bool has_top, D ct0, D ct1) {
-  const D c1 = RN<D>::add(c, D(1));
-  D s = D(0);
-#pragma unroll
-  for (int k = 0; k < 3; k++) {
-    D xs = g.xa[k], xe = g.xb[k];
-    xs = xs > c ? xs : c;
-    xs = xs < c1 ? xs : c1;
-    xe = xe > c ? xe : c;
-    xe = xe < c1 ? xe : c1;
-    const D w = RN<D>::sub(xe, xs);
-    if (w != D(0)) {
-      const D ys = RN<D>::add(g.ya[k], RN<D>::mul(RN<D>::sub(xs, g.xa[k]), t.sl[k]));
-      const D ye = RN<D>::add(g.ya[k], RN<D>::mul(RN<D>::sub(xe, g.xa[k]), t.sl[k]));
-      s = RN<D>::sub(s, RN<D>::mul(RN<D>::mul(w, RN<D>::add(ys, ye)), D(0.5)));
-    }
-  }
-  if (has_top) {
-    D lo = ct0 > c ? ct0 : c, hi = ct1 < c1 ? ct1 : c1;
-    if (hi > lo) s = RN<D>::add(s, RN<D>::sub(hi, lo));
-  }
-  return s;
-}
-
-// One row of a triangle: the run of fully covered pixels goes to the
-// difference array, the other overlapped pixels get their coverage.
+// One row of a triangle: its three edges into the row's difference array.
 template <typename D>
 __device__ __forceinline__ void deposit_row(const Tri<D>& t, int r, int npx, DepositMaps M) {
   const D rb = D(r), rt = D(r + 1);
-  Strip<D> g;
-  D xlo, xhi, cb0, cb1, ct0, ct1;
-  bool hb, ht;
-  if (!row_geometry(t, rb, rt, g, xlo, xhi, hb, cb0, cb1, ht, ct0, ct1)) return;
-  const int cmap_lo = -t.ox, cmap_hi = npx - 1 - t.ox;  // columns inside the map (relative)
-  int cmin = int(floor(xlo)), cmax = int(floor(xhi));
-  if (cmin < cmap_lo) cmin = cmap_lo;
-  if (cmax > cmap_hi) cmax = cmap_hi;
-  if (cmin > cmax) return;
-  int xa = 1, xb = 0;  // full run [xa, xb)
-  if (hb && ht) {
-    D l = cb0 > ct0 ? cb0 : ct0, h = cb1 < ct1 ? cb1 : ct1;
-    xa = int(ceil(l));
-    xb = int(floor(h));
-    if (xa < cmap_lo) xa = cmap_lo;
-    if (xb > cmap_hi + 1) xb = cmap_hi + 1;
-  }
+  const D pb = RN<D>::mul(rb, t.scale), pt = RN<D>::mul(rt, t.scale);
   const long long row = (long long)t.oy + r;
-  const long long rbase = row * npx + t.ox;
-  if (xa < xb) {
-    const unsigned long long q = RN<D>::to_fix(t.scale);
-    const long long dbase = row * ((long long)npx + 1) + t.ox;
-    atomicAdd(M.diff + dbase + xa, q);
-    atomicAdd(M.diff + dbase + xb, (unsigned long long)(0ULL - q));
+  RowAdds out;
+  out.drow = M.diff + row * ((long long)npx + 1) + t.ox;
+  out.chi = npx - t.ox;
+  const int clo = -t.ox;
+  // one copy of the edge code, the edge's values selected by k (no indexed
+  // access, so the triangle stays in registers)
+#pragma unroll 1
+  for (int k = 0; k < 3; k++) {
+    const D xk = k == 0 ? t.x[0] : (k == 1 ? t.x[1] : t.x[2]);
+    const D yk = k == 0 ? t.y[0] : (k == 1 ? t.y[1] : t.y[2]);
+    const D xj = k == 0 ? t.x[1] : (k == 1 ? t.x[2] : t.x[0]);
+    const D yj = k == 0 ? t.y[1] : (k == 1 ? t.y[2] : t.y[0]);
+    const D pk = k == 0 ? t.pv[0] : (k == 1 ? t.pv[1] : t.pv[2]);
+    const D pj = k == 0 ? t.pv[1] : (k == 1 ? t.pv[2] : t.pv[0]);
+    const D g = k == 0 ? t.gxy[0] : (k == 1 ? t.gxy[1] : t.gxy[2]);
+    const D h = k == 0 ? t.gyx[0] : (k == 1 ? t.gyx[1] : t.gyx[2]);
+    deposit_edge_row<D>(xk, yk, xj, yj, pk, pj, g, h, t.scale, rb, rt, pb, pt, clo, out.chi, out);
   }
-  for (int c = cmin; c <= cmax; c++) {
-    if (xa < xb && c == xa) {
-      c = xb - 1;
-      continue;
-    }
-    D a = pixel_coverage(t, g, D(c), ht, ct0, ct1);
-    if (a > D(0)) {
-      unsigned long long q = RN<D>::to_fix(RN<D>::mul(a, t.scale));
-      if (q) atomicAdd(M.acc + rbase + c, q);
-    }
-  }
+  out.flush();
 }
 
 // The rows of the triangles of a warp, one triangle per lane (nrows = 0: none):
@@ -393,8 +416,9 @@ __device__ __forceinline__ void deposit_rows_warp(const Tri<D>& mine, int npx, c
     for (int q = 0; q < 3; q++) {
       t.x[q] = __shfl_sync(0xffffffffu, mine.x[q], owner);
       t.y[q] = __shfl_sync(0xffffffffu, mine.y[q], owner);
-      t.sl[q] = __shfl_sync(0xffffffffu, mine.sl[q], owner);
-      t.idy[q] = __shfl_sync(0xffffffffu, mine.idy[q], owner);
+      t.pv[q] = __shfl_sync(0xffffffffu, mine.pv[q], owner);
+      t.gxy[q] = __shfl_sync(0xffffffffu, mine.gxy[q], owner);
+      t.gyx[q] = __shfl_sync(0xffffffffu, mine.gyx[q], owner);
     }
     t.scale = __shfl_sync(0xffffffffu, mine.scale, owner);
     t.ox = __shfl_sync(0xffffffffu, mine.ox, owner);
@@ -551,6 +575,14 @@ __global__ void __launch_bounds__(kDepositWarps * 32, sizeof(D) == 4 ? 4 : 2)
   }
 }
 
+// Fixed point (modulo 2^64, read as signed) -> magnification: the rounding of
+// the pieces of a pixel's coverage can leave a few units below zero where its
+// true coverage is zero or nearly so; those read as 0.
+__device__ __forceinline__ double fix_to_double(unsigned long long v) {
+  const long long s = (long long)v;
+  return s > 0 ? double(s) * kFixInv : 0.0;
+}
+
 // Row prefix sum of the difference array added to the pieces: one warp per
 // row, 32 columns per step with a carried running sum (integer, exact).
 __global__ void ipm_resolve_rows(int npx, int npy, DepositMaps m) {
@@ -606,7 +638,7 @@ __global__ void ipm_resolve_rows_out(int npx, int npy, DepositMaps m, T* __restr
           const long long k = (long long)y * npx + x + i;
           const unsigned long long v = m.acc[k] + (base + d[i]);
           m.acc[k] = v;
-          out[k] = T(double(v) * kFixInv);
+          out[k] = T(fix_to_double(v));
         }
       }
       carry += __shfl_sync(0xffffffffu, incl, 31);
@@ -623,11 +655,11 @@ __global__ void ipm_finalize(long long n, const unsigned long long* __restrict__
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
     if (parities) {
       unsigned long long a = acc_min[k], b = acc_sad[k];
-      out_min[k] = T(double(a) * kFixInv);
-      out_sad[k] = T(double(b) * kFixInv);
-      out_total[k] = T(double(a + b) * kFixInv);
+      out_min[k] = T(fix_to_double(a));
+      out_sad[k] = T(fix_to_double(b));
+      out_total[k] = T(fix_to_double(a + b));
     } else {
-      out_total[k] = T(double(acc_total[k]) * kFixInv);
+      out_total[k] = T(fix_to_double(acc_total[k]));
     }
   }
 }

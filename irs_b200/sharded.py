@@ -85,7 +85,8 @@ def sharded_run(maker, group=None):
         maps = [reduce_integer_map(h.astype(integer_map_dtype(kind)), group) for h in host]
     if kind == "ipm":
         T = np.float64 if maker.is_double else np.float32
-        maps = [(m.astype(np.float64) / 2.0 ** 32).astype(T) for m in maps]
+        # modulo 2^64, read as signed; a few units below zero read as 0
+        maps = [(np.maximum(m.view(np.int64), 0).astype(np.float64) / 2.0 ** 32).astype(T) for m in maps]
     if par:
         return maps[0] + maps[1], maps[0], maps[1]
     return maps[0], None, None

@@ -174,6 +174,13 @@ def ipm_deposit_fixed(verts, factor, npix, parities=False, single=True):
     return (mn, ms) if parities else mt
 
 
+def fix_to_float(a):
+    """Fixed-point map (uint64, 2^32 per unit, modulo 2^64) -> float64: read
+    as signed, a few units below zero (rounding where the coverage is zero or
+    nearly so) read as 0, as the GPU's conversion does."""
+    return np.maximum(np.asarray(a).view(np.int64), 0).astype(np.float64) / 2.0 ** 32
+
+
 def derive(kappa, gamma, kstar, theta, mean_mass, mean_mass2, light_loss, rect, safety, center, hly, npix, nry):
     out = np.zeros(14)
     lib().orc_derive(kappa, gamma, kstar, theta, mean_mass, mean_mass2, light_loss, int(rect), safety, center[0],

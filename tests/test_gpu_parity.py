@@ -146,7 +146,7 @@ def test_ipm_deposit_bit_exact(gpu, dbl, parities):
     if parities:
         np.testing.assert_array_equal(got[0], ref[0])
         np.testing.assert_array_equal(got[1], ref[1])
-        tot = (got[0] + got[1]).astype(np.float64) / 2.0 ** 32
+        tot = po.fix_to_float(got[0] + got[1])
         np.testing.assert_allclose(m.magnifications, tot.astype(m.magnifications.dtype), rtol=0, atol=0)
     else:
         np.testing.assert_array_equal(got, ref)

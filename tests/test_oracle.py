@@ -93,7 +93,7 @@ def test_polygon_deposition_matches_reference(gold):
 def test_fixed_point_sweep_close_to_reference_deposition(gold, single):
     v = gold["dep_verts"]
     f = np.float32(gold["dep_factor"]) if single else float(gold["dep_factor"])
-    q = po.ipm_deposit_fixed(v, f, (24, 20), single=single).astype(np.float64) / 2.0 ** 32
+    q = po.fix_to_float(po.ipm_deposit_fixed(v, f, (24, 20), single=single))
     ref = gold["dep_map"]
     tol = 1e-4 if single else 1e-8
     assert np.abs(q - ref).max() <= tol * max(1.0, ref.max())
@@ -103,7 +103,7 @@ def test_fixed_point_conserves_area():
     # a lattice of cells entirely inside the map deposits exactly its area
     rng = np.random.default_rng(1)
     v = np.stack(np.meshgrid(np.linspace(5, 25, 21), np.linspace(4, 30, 27)), -1) + rng.normal(0, 0.2, (27, 21, 2))
-    q = po.ipm_deposit_fixed(v, 1.0, (40, 40), single=False).astype(np.float64) / 2.0 ** 32
+    q = po.fix_to_float(po.ipm_deposit_fixed(v, 1.0, (40, 40), single=False))
     assert abs(q.sum() - 2 * 20 * 26) < 1e-6
 
 
@@ -113,7 +113,7 @@ def test_fixed_point_pixel_aligned_cells(step, single):
     # cell edges exactly on pixel lines (no deflection): an edge on the line
     # between two rows must be counted once
     v = np.stack(np.meshgrid(np.arange(5, 26, step), np.arange(4, 31, step)), -1)
-    q = po.ipm_deposit_fixed(v, 1.0, (40, 40), single=single).astype(np.float64) / 2.0 ** 32
+    q = po.fix_to_float(po.ipm_deposit_fixed(v, 1.0, (40, 40), single=single))
     ref = po.ipm_deposit_ref(v, 1.0, (40, 40))
     np.testing.assert_array_equal(q, ref)
 
