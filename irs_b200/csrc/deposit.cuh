@@ -154,6 +154,25 @@ __device__ __forceinline__ Tri<D> setup_head(double ax, double ay, double bx, do
   t.scale = whole;  // setup_tail turns it into the fixed-point scale
   t.ox = ox;
   t.oy = oy;
+  // a sliver too thin for the fixed point (its heights times the scale
+  // factor * 2^32 / area would pass 2^61): its whole flux at the pixel of its
+  // centroid, if that is on the map
+  const D ylim = mxy > D(1) ? mxy : D(1);
+  if (whole < RN<D>::mul(RN<D>::mul(factor, ylim), D(1.0 / 536870912.0))) {
+    const D third = D(1.0 / 3.0);
+    D gx = RN<D>::mul(RN<D>::add(RN<D>::add(x0, x1), x2), third);
+    D gy = RN<D>::mul(RN<D>::add(RN<D>::add(y0, y1), y2), third);
+    gx = gx < X1 ? gx : X1;  // only whether it is on the map matters beyond the map's edge
+    gy = gy < Y1 ? gy : Y1;
+    const int px = ox + int(floor(gx)), py = oy + int(floor(gy));
+    if (px >= 0 && px < npx && py >= 0 && py < npy) {
+      t.ox = px;
+      t.oy = py;
+      t.nrows = 1;
+      t.single = 1;
+    }
+    return t;
+  }
   int rlo = 0 > -oy ? 0 : -oy;
   int rhi = mxy < D(npy - oy) ? int(floor(mxy)) : npy - 1 - oy;
   t.rlo = rlo;
