@@ -198,96 +198,73 @@ __device__ __forceinline__ void setup_tail(Tri<D>& t, D factor) {
   }
 }
 
-// Shared-memory staging of the 64 triangles of a warp's 32 cells that go row
-// by row (one array per field: lane k touches word k, no bank conflicts).
+// Shared-memory staging of the (at most 32) prepared triangles of one half of
+// a warp's 32 cells that go row by row: one array per field, slot s of field
+// f at f[s] (lanes reading distinct slots hit distinct banks; lanes reading
+// one slot get a broadcast).
 template <typename D>
-struct TriSlots {
-  D x[3][64], y[3][64], area[64];
-  int ox[64], oy[64], rlo[64], nrows[64], map[64];
-  __device__ __forceinline__ void put(int k, const Tri<D>& t) {
+struct TriStage {
+  D x[3][32], y[3][32], pv[3][32], gxy[3][32], gyx[3][32], scale[32];
+  int ox[32], oy[32], rlo[32], nrows[32], map[32];
+  __device__ __forceinline__ void put(int s, const Tri<D>& t) {
 #pragma unroll
     for (int q = 0; q < 3; q++) {
-      x[q][k] = t.x[q];
-      y[q][k] = t.y[q];
+      x[q][s] = t.x[q];
+      y[q][s] = t.y[q];
+      pv[q][s] = t.pv[q];
+      gxy[q][s] = t.gxy[q];
+      gyx[q][s] = t.gyx[q];
     }
-    area[k] = t.scale;
-    ox[k] = t.ox;
-    oy[k] = t.oy;
-    rlo[k] = t.rlo;
-    nrows[k] = t.nrows;
-    map[k] = t.map;
-  }
-  __device__ __forceinline__ void get(int k, Tri<D>& t) const {
-#pragma unroll
-    for (int q = 0; q < 3; q++) {
-      t.x[q] = x[q][k];
-      t.y[q] = y[q][k];
-    }
-    t.scale = area[k];
-    t.ox = ox[k];
-    t.oy = oy[k];
-    t.rlo = rlo[k];
-    t.nrows = nrows[k];
-    t.map = map[k];
-    t.single = 0;
+    scale[s] = t.scale;
+    ox[s] = t.ox;
+    oy[s] = t.oy;
+    rlo[s] = t.rlo;
+    nrows[s] = t.nrows;
+    map[s] = t.map;
   }
 };
 constexpr int kDepositWarps = 8;  // warps per CTA of the deposition kernels (256 threads)
 
-// Difference-array adds of one row, merged while consecutive adds hit the
-// same column (the shared column of two neighbouring pieces of an edge).
-// Columns are relative to the triangle's origin; those at or right of the
-// map's last column + 1 (chi) are dropped.
-struct RowAdds {
-  unsigned long long* drow;  // difference-array row at relative column 0
-  int chi;
-  int idx = -(1 << 30);
-  unsigned long long val = 0;
-  __device__ __forceinline__ void flush() {
-    if (idx < chi && val) atomicAdd(drow + idx, val);
-  }
-  __device__ __forceinline__ void add(int c, unsigned long long v) {
-    if (c != idx) {
-      flush();
-      idx = c;
-      val = v;
-    } else {
-      val += v;
-    }
-  }
-};
+// Fire-and-forget 64-bit add to global memory (the map's difference array).
+__device__ __forceinline__ void red_add(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.global.add.u64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v) : "memory");
+}
 
-// Edge (xk, yk) -> (xj, yj) of a triangle inside row strip [rb, rt = rb + 1]
-// (relative): the pieces between its entry and exit points, split at the
-// column lines, into the row's difference array. pvk, pvj: the vertices'
-// heights times the scale; g = dx/dy, h = dy/dx of the edge; pb, pt: rb and
-// rt times the scale. Columns left of the map (relative column clo) are
-// merged into one cover at clo; the part right of column chi is dropped.
+// Edge k of staged triangle s inside row strip [rb, rt = rb + 1] (relative):
+// the pieces between its entry and exit points, split at the column lines,
+// into the row's difference array drow (relative column c at drow[c]). Each
+// piece in column c adds a0 = K - a1 at c and a1 at c + 1; the add shared by
+// two neighbouring pieces is made once. pb, pt: rb and rt times the scale.
+// Columns left of the map (relative column clo) are merged into one cover at
+// clo; the part right of column chi is dropped.
 template <typename D>
-__device__ __forceinline__ void deposit_edge_row(D xk, D yk, D xj, D yj, D pvk, D pvj, D g, D h, D scale, D rb,
-                                                 D rt, D pb, D pt, int clo, int chi, RowAdds& out) {
+__device__ __forceinline__ void deposit_edge_row(const TriStage<D>& st, int s, int k, D scale, D rb, D rt, D pb, D pt,
+                                                 int clo, int chi, unsigned long long* drow) {
+  const int j = k == 2 ? 0 : k + 1;
+  const D yk = st.y[k][s], yj = st.y[j][s];
   if (yk == yj) return;  // a horizontal edge has no cover
   const D ylo = yk < yj ? yk : yj, yhi = yk > yj ? yk : yj;
   if (!(ylo < rt && yhi > rb)) return;
+  const D xk = st.x[k][s], xj = st.x[j][s];
   const D xlo = xk < xj ? xk : xj, xhi = xk > xj ? xk : xj;
   // entry (a) and exit (b) of the edge in the strip, in the edge's direction:
   // a vertex, or the crossing with a row line (x from the edge, y exact)
   D xa, ya, qa, xb, yb, qb;
   const bool up = yj > yk;
   const D ea = up ? rb : rt, eb = up ? rt : rb;  // row lines where the edge enters / leaves
-  const D pea = up ? pb : pt, peb = up ? pt : pb;
   if (up ? (yk >= rb) : (yk <= rt)) {
-    xa = xk, ya = yk, qa = pvk;
+    xa = xk, ya = yk, qa = st.pv[k][s];
   } else {
-    const D x = RN<D>::add(xk, RN<D>::mul(RN<D>::sub(ea, yk), g));
-    xa = x < xlo ? xlo : (x > xhi ? xhi : x), ya = ea, qa = pea;
+    const D x = RN<D>::add(xk, RN<D>::mul(RN<D>::sub(ea, yk), st.gxy[k][s]));
+    xa = x < xlo ? xlo : (x > xhi ? xhi : x), ya = ea, qa = up ? pb : pt;
   }
   if (up ? (yj <= rt) : (yj >= rb)) {
-    xb = xj, yb = yj, qb = pvj;
+    xb = xj, yb = yj, qb = st.pv[j][s];
   } else {
-    const D x = RN<D>::add(xk, RN<D>::mul(RN<D>::sub(eb, yk), g));
-    xb = x < xlo ? xlo : (x > xhi ? xhi : x), yb = eb, qb = peb;
+    const D x = RN<D>::add(xk, RN<D>::mul(RN<D>::sub(eb, yk), st.gxy[k][s]));
+    xb = x < xlo ? xlo : (x > xhi ? xhi : x), yb = eb, qb = up ? pt : pb;
   }
+  const D h = st.gyx[k][s];
   const D plo = ya < yb ? ya : yb, phi = ya > yb ? ya : yb;
   // height (times scale) where the edge crosses the column line X, kept inside the piece's range
   auto cross = [&](D X) {
@@ -309,9 +286,10 @@ __device__ __forceinline__ void deposit_edge_row(D xk, D yk, D xj, D yj, D pvk, 
   }
   long long fa = (long long)RN<D>::to_fix(qa);
   long long fb = (long long)RN<D>::to_fix(qb);
+  unsigned long long carry = 0;  // pending add at the column shared with the next piece
   if (dir >= 0) {
     if (ce < clo) {  // all of it left of the map
-      out.add(clo, (unsigned long long)(fa - fb));
+      red_add(drow + clo, (unsigned long long)(fa - fb));
       return;
     }
     if (c >= chi) return;
@@ -319,7 +297,7 @@ __device__ __forceinline__ void deposit_edge_row(D xk, D yk, D xj, D yj, D pvk, 
       const D X = D(clo);
       const D q = cross(X);
       const long long f = (long long)RN<D>::to_fix(q);
-      out.add(clo, (unsigned long long)(fa - f));
+      carry = (unsigned long long)(fa - f);
       xa = X, qa = q, fa = f, c = clo;
     }
     if (ce >= chi) {  // stop at the map's right edge
@@ -328,7 +306,7 @@ __device__ __forceinline__ void deposit_edge_row(D xk, D yk, D xj, D yj, D pvk, 
     }
   } else {
     if (c < clo) {
-      out.add(clo, (unsigned long long)(fa - fb));
+      red_add(drow + clo, (unsigned long long)(fa - fb));
       return;
     }
     if (ce >= chi) return;
@@ -339,12 +317,13 @@ __device__ __forceinline__ void deposit_edge_row(D xk, D yk, D xj, D yj, D pvk, 
   }
   const bool left_tail = dir < 0 && ce < clo;  // leftward past the map's first column
   const int cstop = left_tail ? clo : ce;
+  const bool rightward = dir >= 0;
   for (;;) {
     const bool last = c == cstop;
     D xq, qq;
     long long fq;
     if (!last || left_tail) {
-      xq = D(dir > 0 ? c + 1 : c);  // the column line where the piece leaves column c
+      xq = D(rightward ? c + 1 : c);  // the column line where the piece leaves column c
       qq = cross(xq);
       fq = (long long)RN<D>::to_fix(qq);
     } else {
@@ -355,109 +334,51 @@ __device__ __forceinline__ void deposit_edge_row(D xk, D yk, D xj, D yj, D pvk, 
     fm = fm < D(0) ? D(0) : (fm > D(1) ? D(1) : fm);
     const long long a1 = (long long)RN<D>::to_fix(RN<D>::mul(RN<D>::sub(qa, qq), fm));
     const long long a0 = K - a1;
-    if (dir >= 0) {
-      out.add(c, (unsigned long long)a0);
-      out.add(c + 1, (unsigned long long)a1);
-    } else {
-      out.add(c + 1, (unsigned long long)a1);
-      out.add(c, (unsigned long long)a0);
-    }
+    // rightward: column c gets the carry and a0, a1 is carried to c + 1;
+    // leftward: column c + 1 gets the carry and a1, a0 is carried to c
+    const int near = rightward ? c : c + 1;
+    const unsigned long long v = carry + (unsigned long long)(rightward ? a0 : a1);
+    carry = (unsigned long long)(rightward ? a1 : a0);
+    if (near < chi && v) red_add(drow + near, v);
     xa = xq, qa = qq, fa = fq;
     if (last) break;
     c += dir;
   }
-  if (left_tail) out.add(clo, (unsigned long long)(fa - fb));
+  if (left_tail) carry += (unsigned long long)(fa - fb);
+  const int far = rightward ? c + 1 : c;
+  if (far < chi && carry) red_add(drow + far, carry);
 }
 
-// One row of a triangle: its three edges into the row's difference array.
+// Row r (relative) of staged triangle s: its three edges into the row's
+// difference array.
 template <typename D>
-__device__ __forceinline__ void deposit_row(const Tri<D>& t, int r, int npx, DepositMaps M) {
+__device__ __forceinline__ void deposit_row(const TriStage<D>& st, int s, int r, int npx, const DepositMaps& m_total,
+                                            const DepositMaps& m_min, const DepositMaps& m_sad) {
+  const D scale = st.scale[s];
+  const int ox = st.ox[s], oy = st.oy[s], map = st.map[s];
   const D rb = D(r), rt = D(r + 1);
-  const D pb = RN<D>::mul(rb, t.scale), pt = RN<D>::mul(rt, t.scale);
-  const long long row = (long long)t.oy + r;
-  RowAdds out;
-  out.drow = M.diff + row * ((long long)npx + 1) + t.ox;
-  out.chi = npx - t.ox;
-  const int clo = -t.ox;
-  // one copy of the edge code, the edge's values selected by k (no indexed
-  // access, so the triangle stays in registers)
+  const D pb = RN<D>::mul(rb, scale), pt = RN<D>::mul(rt, scale);
+  const DepositMaps& M = map == 0 ? m_total : (map == 1 ? m_min : m_sad);
+  unsigned long long* drow = M.diff + ((long long)oy + r) * ((long long)npx + 1) + ox;
+  const int clo = -ox, chi = npx - ox;
 #pragma unroll 1
-  for (int k = 0; k < 3; k++) {
-    const D xk = k == 0 ? t.x[0] : (k == 1 ? t.x[1] : t.x[2]);
-    const D yk = k == 0 ? t.y[0] : (k == 1 ? t.y[1] : t.y[2]);
-    const D xj = k == 0 ? t.x[1] : (k == 1 ? t.x[2] : t.x[0]);
-    const D yj = k == 0 ? t.y[1] : (k == 1 ? t.y[2] : t.y[0]);
-    const D pk = k == 0 ? t.pv[0] : (k == 1 ? t.pv[1] : t.pv[2]);
-    const D pj = k == 0 ? t.pv[1] : (k == 1 ? t.pv[2] : t.pv[0]);
-    const D g = k == 0 ? t.gxy[0] : (k == 1 ? t.gxy[1] : t.gxy[2]);
-    const D h = k == 0 ? t.gyx[0] : (k == 1 ? t.gyx[1] : t.gyx[2]);
-    deposit_edge_row<D>(xk, yk, xj, yj, pk, pj, g, h, t.scale, rb, rt, pb, pt, clo, out.chi, out);
-  }
-  out.flush();
-}
-
-// The rows of the triangles of a warp, one triangle per lane (nrows = 0: none):
-// each lane deposits its own triangle's first row; the warp then scans the
-// counts of the remaining rows and works through those (triangle, row) items
-// 32 at a time, each lane finding its item's owner lane by a binary search
-// over the scan and reading the triangle through shuffles, so a triangle with
-// many rows is spread over the warp instead of holding one lane.
-template <typename D>
-__device__ __forceinline__ void deposit_rows_warp(const Tri<D>& mine, int npx, const DepositMaps& m_total,
-                                                  const DepositMaps& m_min, const DepositMaps& m_sad) {
-  const int lane = threadIdx.x & 31;
-  if (mine.nrows > 0) {
-    const DepositMaps& M = mine.map == 0 ? m_total : (mine.map == 1 ? m_min : m_sad);
-    deposit_row<D>(mine, mine.rlo, npx, M);
-  }
-  const int extra = mine.nrows > 1 ? mine.nrows - 1 : 0;
-  int incl = extra;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int v = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += v;
-  }
-  const int total = __shfl_sync(0xffffffffu, incl, 31);
-  for (int it0 = 0; it0 < total; it0 += 32) {
-    const int item = it0 + lane;
-    int lo = 0, hi = 31;  // owner: first lane whose inclusive count exceeds item
-#pragma unroll
-    for (int step = 0; step < 5; step++) {
-      int mid = (lo + hi) >> 1;
-      int v = __shfl_sync(0xffffffffu, incl, mid);
-      if (v > item) hi = mid;
-      else lo = mid + 1;
-    }
-    const int owner = lo;
-    const int before = __shfl_sync(0xffffffffu, incl - extra, owner);
-    Tri<D> t;
-#pragma unroll
-    for (int q = 0; q < 3; q++) {
-      t.x[q] = __shfl_sync(0xffffffffu, mine.x[q], owner);
-      t.y[q] = __shfl_sync(0xffffffffu, mine.y[q], owner);
-      t.pv[q] = __shfl_sync(0xffffffffu, mine.pv[q], owner);
-      t.gxy[q] = __shfl_sync(0xffffffffu, mine.gxy[q], owner);
-      t.gyx[q] = __shfl_sync(0xffffffffu, mine.gyx[q], owner);
-    }
-    t.scale = __shfl_sync(0xffffffffu, mine.scale, owner);
-    t.ox = __shfl_sync(0xffffffffu, mine.ox, owner);
-    t.oy = __shfl_sync(0xffffffffu, mine.oy, owner);
-    t.rlo = __shfl_sync(0xffffffffu, mine.rlo, owner);
-    t.map = __shfl_sync(0xffffffffu, mine.map, owner);
-    if (item < total) {
-      const DepositMaps& M = t.map == 0 ? m_total : (t.map == 1 ? m_min : m_sad);
-      deposit_row<D>(t, t.rlo + 1 + (item - before), npx, M);
-    }
-  }
+  for (int k = 0; k < 3; k++) deposit_edge_row<D>(st, s, k, scale, rb, rt, pb, pt, clo, chi, drow);
 }
 
 // The 32 cells [base, base + 32) of an ncx-wide lattice whose corner rows are
-// vx apart (whole warp; lanes past ncells idle).
+// vx apart (whole warp; lanes past ncells idle). For each half of the cells
+// (the triangles (y0, y1, y2), then (y2, y3, y0)): each lane classifies its
+// triangle (setup_head); a triangle inside one pixel deposits at once, lanes
+// in a row whose triangles fall in the same pixel adding once for all of
+// them; the others are prepared (setup_tail) and staged in shared memory,
+// compacted in lane order; the warp then scans their row counts and works
+// through the (triangle, row) items 32 at a time, each lane finding its
+// item's triangle by a binary search over the scan.
 template <typename D>
 __device__ __forceinline__ void deposit_warp_cells(const double2* __restrict__ verts, long long ncx, long long vx,
                                                    long long ncells, long long base, D factor, int npx, int npy,
                                                    const DepositMaps& m_total, const DepositMaps& m_min,
-                                                   const DepositMaps& m_sad, int parities, TriSlots<D>& stage,
+                                                   const DepositMaps& m_sad, int parities, TriStage<D>& stage,
                                                    long long vstep = 1, double ox = 0.0, double oy = 0.0,
                                                    double inv_scale = 1.0) {
   const int lane = threadIdx.x & 31;
@@ -486,10 +407,7 @@ __device__ __forceinline__ void deposit_warp_cells(const double2* __restrict__ v
       y0.y *= inv_scale, y1.y *= inv_scale, y2.y *= inv_scale, y3.y *= inv_scale;
     }
   }
-  // each half's head: a triangle inside one pixel deposits at once, the
-  // others are staged in the warp's slots, compacted in lane order
   const unsigned lt = (1u << lane) - 1u;
-  int n = 0;
 #pragma unroll 1
   for (int half = 0; half < 2; half++) {
     Tri<D> h;
@@ -510,36 +428,46 @@ __device__ __forceinline__ void deposit_warp_cells(const double2* __restrict__ v
       if (h.single && (starts >> lane & 1u)) {
         const unsigned later = starts & ~((2u << lane) - 1u);  // lane 31: mask of all bits, none later
         const int end = later ? __ffs(later) - 1 : 32;
-        atomicAdd(a, (unsigned long long)(end - lane) * RN<D>::to_fix(RN<D>::mul(factor, D(kFixScale))));
+        red_add(a, (unsigned long long)(end - lane) * RN<D>::to_fix(RN<D>::mul(factor, D(kFixScale))));
       }
     }
-    const bool cx = h.nrows > 0 && !h.single;
-    const unsigned b = __ballot_sync(0xffffffffu, cx);
-    if (cx) stage.put(n + __popc(b & lt), h);
-    n += __popc(b);
-  }
-  __syncwarp();
-  // the staged ones go row by row, one per lane: one round when at most 32
-  // of the warp's 64 triangles need it (fine lattices), else two
-  for (int r0 = 0; r0 < n; r0 += 32) {
-    Tri<D> mine;
-    mine.nrows = 0;
-    if (r0 + lane < n) {
-      stage.get(r0 + lane, mine);
-      setup_tail(mine, factor);
+    const bool rows = h.nrows > 0 && !h.single;
+    const unsigned b = __ballot_sync(0xffffffffu, rows);
+    if (b == 0u) continue;
+    const int slot = __popc(b & lt);
+    if (rows) {
+      setup_tail(h, factor);
+      stage.put(slot, h);
     }
-    deposit_rows_warp<D>(mine, npx, m_total, m_min, m_sad);
+    __syncwarp();
+    // inclusive scan of the staged triangles' row counts, lane s holding slot s
+    const int mycnt = lane < __popc(b) ? stage.nrows[lane] : 0;
+    int incl = mycnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    for (int it0 = 0; it0 < total; it0 += 32) {
+      const int item = it0 + lane;
+      int lo = 0, hi = 31;  // slot: first lane whose inclusive count exceeds item
+#pragma unroll
+      for (int step = 0; step < 5; step++) {
+        const int mid = (lo + hi) >> 1;
+        const int v = __shfl_sync(0xffffffffu, incl, mid);
+        if (v > item) hi = mid;
+        else lo = mid + 1;
+      }
+      const int before = __shfl_sync(0xffffffffu, incl - mycnt, lo);
+      if (item < total) deposit_row<D>(stage, lo, stage.rlo[lo] + (item - before), npx, m_total, m_min, m_sad);
+    }
+    __syncwarp();  // slots free for the next half
   }
-  __syncwarp();  // slots free for the warp's next cells
 }
 
 // Cells of an ncx x ncy lattice whose (ncx+1) x (ncy+1) corner positions are in
-// `verts`. A warp takes 32 consecutive cells; each lane classifies the two
-// triangles of its cell (setup_head); a triangle inside one pixel is
-// deposited at once; the others are staged in shared memory, compacted, and
-// then get their reciprocals and scale (setup_tail) and go row by row
-// (deposit_rows_warp), one per lane: one round when at most 32 of the warp's
-// 64 triangles need it (fine lattices), else two.
+// `verts`, 32 consecutive cells per warp (deposit_warp_cells).
 template <typename D>
 __global__ void __launch_bounds__(kDepositWarps * 32, sizeof(D) == 4 ? 4 : 2)
     ipm_deposit_cells(const double2* __restrict__ verts, long long ncx, long long ncy, D factor, int npx, int npy,
@@ -547,8 +475,8 @@ __global__ void __launch_bounds__(kDepositWarps * 32, sizeof(D) == 4 ? 4 : 2)
   const long long ncells = ncx * ncy;
   const long long warp0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  __shared__ TriSlots<D> slots[kDepositWarps];
-  TriSlots<D>& stage = slots[threadIdx.x >> 5];
+  __shared__ TriStage<D> stages[kDepositWarps];
+  TriStage<D>& stage = stages[threadIdx.x >> 5];
   for (long long base = warp0 * 32; base < ncells; base += nwarps * 32)
     deposit_warp_cells<D>(verts, ncx, ncx + 1, ncells, base, factor, npx, npy, m_total, m_min, m_sad, parities, stage);
 }
@@ -578,8 +506,8 @@ __global__ void __launch_bounds__(kDepositWarps * 32, sizeof(D) == 4 ? 4 : 2)
                       long long diff_stride) {
   const long long warp0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  __shared__ TriSlots<D> slots[kDepositWarps];
-  TriSlots<D>& stage = slots[threadIdx.x >> 5];
+  __shared__ TriStage<D> stages[kDepositWarps];
+  TriStage<D>& stage = stages[threadIdx.x >> 5];
   for (long long g = warp0; g < nchunks; g += nwarps) {
     int lo = 0, hi = npieces - 1;  // last piece with chunk0 <= g
     while (lo < hi) {
