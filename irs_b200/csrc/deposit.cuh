@@ -10,27 +10,20 @@
 // factor * |A ∩ pixel| / |A|.
 //
 // How, differently by design:
-//   * no polygon clipping: each triangle's area is spread over the pixels by
-//     accumulating its edges into a per-row difference array (a coverage
-//     accumulation rasterizer). An edge piece lying inside pixel column c of
-//     row strip r, running from height ya to yb, contributes the cover
-//     K = F(ya) - F(yb) to every pixel right of c and the share
-//     K (1 - f) to pixel c itself, f being the piece's mean x inside the
-//     column; in the difference array that is K - a1 at c and a1 = round(K f)
-//     at c + 1, so that the row's prefix sum gives each pixel's covered area.
-//     F(y) = round(y * scale) is evaluated once per break point (a vertex, a
-//     crossing of a row line or of a column line) and shared by the two pieces
-//     meeting there, so the covers of every row of a triangle sum to exactly
-//     zero: nothing leaks right of a triangle, whatever the rounding;
+//   * the overlap of a triangle with a pixel is computed directly from
+//     Green's theorem instead of by successive polygon clips: the edges are
+//     clipped once per row strip (row_geometry), and each pixel of the row
+//     then only clamps those segments to its column (pixel_coverage):
+//     register-only arithmetic, no polygon arrays;
 //   * rows of a triangle are independent work items; a warp expands the rows
 //     of its 64 triangles and shares them out 32 at a time;
-//   * pieces left of the map are merged into one cover at the map's first
-//     column; pieces right of it are dropped;
+//   * pixels inside both the bottom and the top chord of a row strip are fully
+//     covered (area exactly 1) and are added as a run through a per-row
+//     difference array;
 //   * coordinates are relative to an integer origin at the triangle's
-//     lower-left pixel; the map accumulates 64-bit fixed point (2^32 per unit,
-//     modulo 2^64, read as signed) with integer atomics, so the result does not
-//     depend on thread order: given the same corner positions the map is
-//     bit-exact.
+//     lower-left pixel; the map accumulates unsigned 64-bit fixed point (2^32
+//     per unit) with integer atomics, so the result does not depend on thread
+//     order: given the same corner positions the map is bit-exact.
 // Every floating-point operation is an explicitly rounded intrinsic (no FMA
 // contraction), so a host implementation with the same operation sequence
 // reproduces the map bit for bit.
@@ -79,14 +72,12 @@ struct DepositMaps {
 };
 
 // A triangle prepared for deposition: CCW vertices relative to the integer
-// origin (ox, oy), per-edge slopes, the vertices' heights times the
-// fixed-point scale, and the target map.
+// origin (ox, oy), per-edge reciprocals, fixed-point scale and target map.
 template <typename D>
 struct Tri {
   D x[3], y[3];     // CCW, relative to (ox, oy)
-  D pv[3];          // y[k] * scale (unrounded): F(y[k]) = round(pv[k])
-  D gxy[3];         // dx * (1 / dy) of edge k -> k+1 (0 for a horizontal edge)
-  D gyx[3];         // dy * (1 / dx) of edge k -> k+1 (0 for a vertical edge or an overflow)
+  D idy[3];         // 1 / (y[k+1] - y[k]) (0 for a zero difference)
+  D sl[3];          // slope (y[k+1] - y[k]) * (1 / (x[k+1] - x[k])); 0 for a vertical edge or an overflow
   D scale;          // factor * 2^32 / |area|
   int ox, oy;
   int rlo, nrows;   // first row (relative) and number of rows to visit
@@ -114,7 +105,7 @@ __device__ __forceinline__ Tri<D> setup_head(double ax, double ay, double bx, do
   t.map = 0;
   t.single = 0;
   t.scale = D(0);
-  for (int k = 0; k < 3; k++) t.x[k] = t.y[k] = t.pv[k] = t.gxy[k] = t.gyx[k] = D(0);
+  for (int k = 0; k < 3; k++) t.x[k] = t.y[k] = t.sl[k] = t.idy[k] = D(0);
   if (isnan(ax) || isnan(ay) || isnan(bx) || isnan(by) || isnan(cx) || isnan(cy)) return t;
   double fx = floor(fmin(ax, fmin(bx, cx)));
   double fy = floor(fmin(ay, fmin(by, cy)));
@@ -154,25 +145,6 @@ __device__ __forceinline__ Tri<D> setup_head(double ax, double ay, double bx, do
   t.scale = whole;  // setup_tail turns it into the fixed-point scale
   t.ox = ox;
   t.oy = oy;
-  // a sliver too thin for the fixed point (its heights times the scale
-  // factor * 2^32 / area would pass 2^61): its whole flux at the pixel of its
-  // centroid, if that is on the map
-  const D ylim = mxy > D(1) ? mxy : D(1);
-  if (whole < RN<D>::mul(RN<D>::mul(factor, ylim), D(1.0 / 536870912.0))) {
-    const D third = D(1.0 / 3.0);
-    D gx = RN<D>::mul(RN<D>::add(RN<D>::add(x0, x1), x2), third);
-    D gy = RN<D>::mul(RN<D>::add(RN<D>::add(y0, y1), y2), third);
-    gx = gx < X1 ? gx : X1;  // only whether it is on the map matters beyond the map's edge
-    gy = gy < Y1 ? gy : Y1;
-    const int px = ox + int(floor(gx)), py = oy + int(floor(gy));
-    if (px >= 0 && px < npx && py >= 0 && py < npy) {
-      t.ox = px;
-      t.oy = py;
-      t.nrows = 1;
-      t.single = 1;
-    }
-    return t;
-  }
   int rlo = 0 > -oy ? 0 : -oy;
   int rhi = mxy < D(npy - oy) ? int(floor(mxy)) : npy - 1 - oy;
   t.rlo = rlo;
@@ -182,203 +154,266 @@ __device__ __forceinline__ Tri<D> setup_head(double ax, double ay, double bx, do
   return t;
 }
 
-// Slopes, scaled vertex heights and the fixed-point scale of a triangle that
+// Edge reciprocals, slopes and the fixed-point scale of a triangle that
 // deposits row by row (nrows > 0, not single).
 template <typename D>
 __device__ __forceinline__ void setup_tail(Tri<D>& t, D factor) {
-  t.scale = RN<D>::div(RN<D>::mul(factor, D(kFixScale)), t.scale);
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     const int j = k == 2 ? 0 : k + 1;
     const D dx = RN<D>::sub(t.x[j], t.x[k]), dy = RN<D>::sub(t.y[j], t.y[k]);
-    t.gxy[k] = RN<D>::mul(dx, rcp_or_zero(dy));
+    t.idy[k] = rcp_or_zero(dy);
     const D g = RN<D>::mul(dy, rcp_or_zero(dx));
-    t.gyx[k] = dabs(g) <= std::numeric_limits<D>::max() ? g : D(0);
-    t.pv[k] = RN<D>::mul(t.y[k], t.scale);
+    t.sl[k] = dabs(g) <= std::numeric_limits<D>::max() ? g : D(0);
   }
+  t.scale = RN<D>::div(RN<D>::mul(factor, D(kFixScale)), t.scale);
 }
 
-// Shared-memory staging of the (at most 32) prepared triangles of one half of
-// a warp's 32 cells that go row by row: one array per field, slot s of field
-// f at f[s] (lanes reading distinct slots hit distinct banks; lanes reading
-// one slot get a broadcast).
+// Shared-memory staging of the 64 triangles of a warp's 32 cells that go row
+// by row (one array per field: lane k touches word k, no bank conflicts).
 template <typename D>
-struct TriStage {
-  D x[3][32], y[3][32], pv[3][32], gxy[3][32], gyx[3][32], scale[32];
-  int ox[32], oy[32], rlo[32], nrows[32], map[32];
-  __device__ __forceinline__ void put(int s, const Tri<D>& t) {
+struct TriSlots {
+  D x[3][64], y[3][64], area[64];
+  int ox[64], oy[64], rlo[64], nrows[64], map[64];
+  __device__ __forceinline__ void put(int k, const Tri<D>& t) {
 #pragma unroll
     for (int q = 0; q < 3; q++) {
-      x[q][s] = t.x[q];
-      y[q][s] = t.y[q];
-      pv[q][s] = t.pv[q];
-      gxy[q][s] = t.gxy[q];
-      gyx[q][s] = t.gyx[q];
+      x[q][k] = t.x[q];
+      y[q][k] = t.y[q];
     }
-    scale[s] = t.scale;
-    ox[s] = t.ox;
-    oy[s] = t.oy;
-    rlo[s] = t.rlo;
-    nrows[s] = t.nrows;
-    map[s] = t.map;
+    area[k] = t.scale;
+    ox[k] = t.ox;
+    oy[k] = t.oy;
+    rlo[k] = t.rlo;
+    nrows[k] = t.nrows;
+    map[k] = t.map;
+  }
+  __device__ __forceinline__ void get(int k, Tri<D>& t) const {
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      t.x[q] = x[q][k];
+      t.y[q] = y[q][k];
+    }
+    t.scale = area[k];
+    t.ox = ox[k];
+    t.oy = oy[k];
+    t.rlo = rlo[k];
+    t.nrows = nrows[k];
+    t.map = map[k];
+    t.single = 0;
   }
 };
 constexpr int kDepositWarps = 8;  // warps per CTA of the deposition kernels (256 threads)
 
-// Fire-and-forget 64-bit add to global memory (the map's difference array).
-__device__ __forceinline__ void red_add(unsigned long long* p, unsigned long long v) {
-  asm volatile("red.global.add.u64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v) : "memory");
+// Geometry of one row strip [rb, rt = rb + 1] of a triangle.
+//   Strip segments: each edge clipped to the strip, endpoints (xa, ya) ->
+//   (xb, yb) with y relative to rb, a zero segment where the edge misses the
+//   strip. A horizontal edge belongs to the strip only on [rb, rt), so an edge
+//   lying on the line between two rows is counted once (by the top chord of
+//   the row below).
+//   Chords: x-extent of the triangle on the lines y = rb and y = rt (an edge
+//   reaching the line contributes its crossing, x1 + ((y - y1) / dy) dx, or
+//   both ends when it lies on the line).
+template <typename D>
+struct Strip {
+  D xa[3], ya[3], xb[3], yb[3];
+};
+
+template <typename D>
+__device__ __forceinline__ void extend(bool& any, D& lo, D& hi, D a, D b) {
+  const D mn = a < b ? a : b, mx = a > b ? a : b;
+  lo = any ? (mn < lo ? mn : lo) : mn;
+  hi = any ? (mx > hi ? mx : hi) : mx;
+  any = true;
 }
 
-// Edge k of staged triangle s inside row strip [rb, rt = rb + 1] (relative):
-// the pieces between its entry and exit points, split at the column lines,
-// into the row's difference array drow (relative column c at drow[c]). Each
-// piece in column c adds a0 = K - a1 at c and a1 at c + 1; the add shared by
-// two neighbouring pieces is made once. pb, pt: rb and rt times the scale.
-// Columns left of the map (relative column clo) are merged into one cover at
-// clo; the part right of column chi is dropped.
+// Fills the strip segments and both chords; returns false when the triangle
+// does not enter the strip, else sets its x-extent [xlo, xhi] there.
 template <typename D>
-__device__ __forceinline__ void deposit_edge_row(const TriStage<D>& st, int s, int k, D scale, D rb, D rt, D pb, D pt,
-                                                 int clo, int chi, unsigned long long* drow) {
-  const int j = k == 2 ? 0 : k + 1;
-  const D yk = st.y[k][s], yj = st.y[j][s];
-  if (yk == yj) return;  // a horizontal edge has no cover
-  const D ylo = yk < yj ? yk : yj, yhi = yk > yj ? yk : yj;
-  if (!(ylo < rt && yhi > rb)) return;
-  const D xk = st.x[k][s], xj = st.x[j][s];
-  const D xlo = xk < xj ? xk : xj, xhi = xk > xj ? xk : xj;
-  // entry (a) and exit (b) of the edge in the strip, in the edge's direction:
-  // a vertex, or the crossing with a row line (x from the edge, y exact)
-  D xa, ya, qa, xb, yb, qb;
-  const bool up = yj > yk;
-  const D ea = up ? rb : rt, eb = up ? rt : rb;  // row lines where the edge enters / leaves
-  if (up ? (yk >= rb) : (yk <= rt)) {
-    xa = xk, ya = yk, qa = st.pv[k][s];
-  } else {
-    const D x = RN<D>::add(xk, RN<D>::mul(RN<D>::sub(ea, yk), st.gxy[k][s]));
-    xa = x < xlo ? xlo : (x > xhi ? xhi : x), ya = ea, qa = up ? pb : pt;
-  }
-  if (up ? (yj <= rt) : (yj >= rb)) {
-    xb = xj, yb = yj, qb = st.pv[j][s];
-  } else {
-    const D x = RN<D>::add(xk, RN<D>::mul(RN<D>::sub(eb, yk), st.gxy[k][s]));
-    xb = x < xlo ? xlo : (x > xhi ? xhi : x), yb = eb, qb = up ? pt : pb;
-  }
-  const D h = st.gyx[k][s];
-  const D plo = ya < yb ? ya : yb, phi = ya > yb ? ya : yb;
-  // height (times scale) where the edge crosses the column line X, kept inside the piece's range
-  auto cross = [&](D X) {
-    D y = RN<D>::add(yk, RN<D>::mul(RN<D>::sub(X, xk), h));
-    y = y < plo ? plo : (y > phi ? phi : y);
-    return RN<D>::mul(y, scale);
-  };
-  // columns visited: right- or leftward from the entry's column to the exit's
-  // (positions beyond the map are clamped first: only their side matters)
-  const D cl = D(clo - 1), ch = D(chi + 1);
-  const D ua = xa < cl ? cl : (xa > ch ? ch : xa), ub = xb < cl ? cl : (xb > ch ? ch : xb);
-  int dir, c, ce;
-  if (xb > xa) {
-    dir = 1, c = int(floor(ua)), ce = int(ceil(ub)) - 1;
-  } else if (xb < xa) {
-    dir = -1, c = int(ceil(ua)) - 1, ce = int(floor(ub));
-  } else {
-    dir = 0, c = ce = int(floor(ua));
-  }
-  long long fa = (long long)RN<D>::to_fix(qa);
-  long long fb = (long long)RN<D>::to_fix(qb);
-  unsigned long long carry = 0;  // pending add at the column shared with the next piece
-  if (dir >= 0) {
-    if (ce < clo) {  // all of it left of the map
-      red_add(drow + clo, (unsigned long long)(fa - fb));
-      return;
-    }
-    if (c >= chi) return;
-    if (c < clo) {  // the part left of the map: one cover at its first column
-      const D X = D(clo);
-      const D q = cross(X);
-      const long long f = (long long)RN<D>::to_fix(q);
-      carry = (unsigned long long)(fa - f);
-      xa = X, qa = q, fa = f, c = clo;
-    }
-    if (ce >= chi) {  // stop at the map's right edge
-      const D X = D(chi);
-      xb = X, qb = cross(X), fb = (long long)RN<D>::to_fix(qb), ce = chi - 1;
-    }
-  } else {
-    if (c < clo) {
-      red_add(drow + clo, (unsigned long long)(fa - fb));
-      return;
-    }
-    if (ce >= chi) return;
-    if (c >= chi) {  // start at the map's right edge
-      const D X = D(chi);
-      xa = X, qa = cross(X), fa = (long long)RN<D>::to_fix(qa), c = chi - 1;
-    }
-  }
-  const bool left_tail = dir < 0 && ce < clo;  // leftward past the map's first column
-  const int cstop = left_tail ? clo : ce;
-  const bool rightward = dir >= 0;
-  for (;;) {
-    const bool last = c == cstop;
-    D xq, qq;
-    long long fq;
-    if (!last || left_tail) {
-      xq = D(rightward ? c + 1 : c);  // the column line where the piece leaves column c
-      qq = cross(xq);
-      fq = (long long)RN<D>::to_fix(qq);
+__device__ __forceinline__ bool row_geometry(const Tri<D>& t, D rb, D rt, Strip<D>& g, D& xlo, D& xhi, bool& hb,
+                                             D& cb0, D& cb1, bool& ht, D& ct0, D& ct1) {
+  bool any = false;
+  xlo = xhi = cb0 = cb1 = ct0 = ct1 = D(0);
+  hb = ht = false;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const int j = k == 2 ? 0 : k + 1;
+    const D x1 = t.x[k], y1 = t.y[k], x2 = t.x[j], y2 = t.y[j];
+    const D dx = RN<D>::sub(x2, x1), dy = RN<D>::sub(y2, y1);
+    const bool on_b = (y1 <= rb && rb <= y2) || (y2 <= rb && rb <= y1);
+    const bool on_t = (y1 <= rt && rt <= y2) || (y2 <= rt && rt <= y1);
+    D t0 = D(0), t1 = D(1);
+    bool ok;
+    if (dy != D(0)) {
+      const D ta = RN<D>::mul(RN<D>::sub(rb, y1), t.idy[k]), tb = RN<D>::mul(RN<D>::sub(rt, y1), t.idy[k]);
+      if (on_b) {
+        const D p = RN<D>::add(x1, RN<D>::mul(ta, dx));
+        extend(hb, cb0, cb1, p, p);
+      }
+      if (on_t) {
+        const D p = RN<D>::add(x1, RN<D>::mul(tb, dx));
+        extend(ht, ct0, ct1, p, p);
+      }
+      const D lo = ta < tb ? ta : tb, hi = ta > tb ? ta : tb;
+      t0 = lo > t0 ? lo : t0;
+      t1 = hi < t1 ? hi : t1;
+      ok = t0 < t1;
     } else {
-      xq = xb, qq = qb, fq = fb;
+      if (on_b) extend(hb, cb0, cb1, x1, x2);
+      if (on_t) extend(ht, ct0, ct1, x1, x2);
+      ok = y1 >= rb && y1 < rt;
     }
-    const long long K = fa - fq;
-    D fm = RN<D>::sub(RN<D>::mul(RN<D>::add(xa, xq), D(0.5)), D(c));
-    fm = fm < D(0) ? D(0) : (fm > D(1) ? D(1) : fm);
-    const long long a1 = (long long)RN<D>::to_fix(RN<D>::mul(RN<D>::sub(qa, qq), fm));
-    const long long a0 = K - a1;
-    // rightward: column c gets the carry and a0, a1 is carried to c + 1;
-    // leftward: column c + 1 gets the carry and a1, a0 is carried to c
-    const int near = rightward ? c : c + 1;
-    const unsigned long long v = carry + (unsigned long long)(rightward ? a0 : a1);
-    carry = (unsigned long long)(rightward ? a1 : a0);
-    if (near < chi && v) red_add(drow + near, v);
-    xa = xq, qa = qq, fa = fq;
-    if (last) break;
-    c += dir;
+    D xa = D(0), ya = D(0), xb = D(0), yb = D(0);
+    if (ok) {
+      xa = RN<D>::add(x1, RN<D>::mul(t0, dx));
+      xb = RN<D>::add(x1, RN<D>::mul(t1, dx));
+      ya = RN<D>::sub(RN<D>::add(y1, RN<D>::mul(t0, dy)), rb);
+      yb = RN<D>::sub(RN<D>::add(y1, RN<D>::mul(t1, dy)), rb);
+      extend(any, xlo, xhi, xa, xb);
+    }
+    g.xa[k] = xa;
+    g.ya[k] = ya;
+    g.xb[k] = xb;
+    g.yb[k] = yb;
   }
-  if (left_tail) carry += (unsigned long long)(fa - fb);
-  const int far = rightward ? c + 1 : c;
-  if (far < chi && carry) red_add(drow + far, carry);
+  return any;
 }
 
-// Row r (relative) of staged triangle s: its three edges into the row's
-// difference array.
+// Area of the triangle inside the pixel [c, c+1] x [rb, rb+1] from Green's
+// theorem, area = -(sum over the boundary of the integral of (y - rb) dx):
+// each strip segment restricted to the column (both ends clamped to
+// [c, c+1], an edge being monotone in x) is a trapezoid; the pixel's top side
+// adds the top chord's length inside the column; the vertical sides and the
+// bottom side add nothing.
 template <typename D>
-__device__ __forceinline__ void deposit_row(const TriStage<D>& st, int s, int r, int npx, const DepositMaps& m_total,
-                                            const DepositMaps& m_min, const DepositMaps& m_sad) {
-  const D scale = st.scale[s];
-  const int ox = st.ox[s], oy = st.oy[s], map = st.map[s];
+__device__ __forceinline__ D pixel_coverage(const Tri<D>& t, const Strip<D>& g, D c, bool has_top, D ct0, D ct1) {
+  const D c1 = RN<D>::add(c, D(1));
+  D s = D(0);
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    D xs = g.xa[k], xe = g.xb[k];
+    xs = xs > c ? xs : c;
+    xs = xs < c1 ? xs : c1;
+    xe = xe > c ? xe : c;
+    xe = xe < c1 ? xe : c1;
+    const D w = RN<D>::sub(xe, xs);
+    if (w != D(0)) {
+      const D ys = RN<D>::add(g.ya[k], RN<D>::mul(RN<D>::sub(xs, g.xa[k]), t.sl[k]));
+      const D ye = RN<D>::add(g.ya[k], RN<D>::mul(RN<D>::sub(xe, g.xa[k]), t.sl[k]));
+      s = RN<D>::sub(s, RN<D>::mul(RN<D>::mul(w, RN<D>::add(ys, ye)), D(0.5)));
+    }
+  }
+  if (has_top) {
+    D lo = ct0 > c ? ct0 : c, hi = ct1 < c1 ? ct1 : c1;
+    if (hi > lo) s = RN<D>::add(s, RN<D>::sub(hi, lo));
+  }
+  return s;
+}
+
+// One row of a triangle: the run of fully covered pixels goes to the
+// difference array, the other overlapped pixels get their coverage.
+template <typename D>
+__device__ __forceinline__ void deposit_row(const Tri<D>& t, int r, int npx, DepositMaps M) {
   const D rb = D(r), rt = D(r + 1);
-  const D pb = RN<D>::mul(rb, scale), pt = RN<D>::mul(rt, scale);
-  const DepositMaps& M = map == 0 ? m_total : (map == 1 ? m_min : m_sad);
-  unsigned long long* drow = M.diff + ((long long)oy + r) * ((long long)npx + 1) + ox;
-  const int clo = -ox, chi = npx - ox;
-#pragma unroll 1
-  for (int k = 0; k < 3; k++) deposit_edge_row<D>(st, s, k, scale, rb, rt, pb, pt, clo, chi, drow);
+  Strip<D> g;
+  D xlo, xhi, cb0, cb1, ct0, ct1;
+  bool hb, ht;
+  if (!row_geometry(t, rb, rt, g, xlo, xhi, hb, cb0, cb1, ht, ct0, ct1)) return;
+  const int cmap_lo = -t.ox, cmap_hi = npx - 1 - t.ox;  // columns inside the map (relative)
+  int cmin = int(floor(xlo)), cmax = int(floor(xhi));
+  if (cmin < cmap_lo) cmin = cmap_lo;
+  if (cmax > cmap_hi) cmax = cmap_hi;
+  if (cmin > cmax) return;
+  int xa = 1, xb = 0;  // full run [xa, xb)
+  if (hb && ht) {
+    D l = cb0 > ct0 ? cb0 : ct0, h = cb1 < ct1 ? cb1 : ct1;
+    xa = int(ceil(l));
+    xb = int(floor(h));
+    if (xa < cmap_lo) xa = cmap_lo;
+    if (xb > cmap_hi + 1) xb = cmap_hi + 1;
+  }
+  const long long row = (long long)t.oy + r;
+  const long long rbase = row * npx + t.ox;
+  if (xa < xb) {
+    const unsigned long long q = RN<D>::to_fix(t.scale);
+    const long long dbase = row * ((long long)npx + 1) + t.ox;
+    atomicAdd(M.diff + dbase + xa, q);
+    atomicAdd(M.diff + dbase + xb, (unsigned long long)(0ULL - q));
+  }
+  for (int c = cmin; c <= cmax; c++) {
+    if (xa < xb && c == xa) {
+      c = xb - 1;
+      continue;
+    }
+    D a = pixel_coverage(t, g, D(c), ht, ct0, ct1);
+    if (a > D(0)) {
+      unsigned long long q = RN<D>::to_fix(RN<D>::mul(a, t.scale));
+      if (q) atomicAdd(M.acc + rbase + c, q);
+    }
+  }
+}
+
+// The rows of the triangles of a warp, one triangle per lane (nrows = 0: none):
+// each lane deposits its own triangle's first row; the warp then scans the
+// counts of the remaining rows and works through those (triangle, row) items
+// 32 at a time, each lane finding its item's owner lane by a binary search
+// over the scan and reading the triangle through shuffles, so a triangle with
+// many rows is spread over the warp instead of holding one lane.
+template <typename D>
+__device__ __forceinline__ void deposit_rows_warp(const Tri<D>& mine, int npx, const DepositMaps& m_total,
+                                                  const DepositMaps& m_min, const DepositMaps& m_sad) {
+  const int lane = threadIdx.x & 31;
+  if (mine.nrows > 0) {
+    const DepositMaps& M = mine.map == 0 ? m_total : (mine.map == 1 ? m_min : m_sad);
+    deposit_row<D>(mine, mine.rlo, npx, M);
+  }
+  const int extra = mine.nrows > 1 ? mine.nrows - 1 : 0;
+  int incl = extra;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  for (int it0 = 0; it0 < total; it0 += 32) {
+    const int item = it0 + lane;
+    int lo = 0, hi = 31;  // owner: first lane whose inclusive count exceeds item
+#pragma unroll
+    for (int step = 0; step < 5; step++) {
+      int mid = (lo + hi) >> 1;
+      int v = __shfl_sync(0xffffffffu, incl, mid);
+      if (v > item) hi = mid;
+      else lo = mid + 1;
+    }
+    const int owner = lo;
+    const int before = __shfl_sync(0xffffffffu, incl - extra, owner);
+    Tri<D> t;
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      t.x[q] = __shfl_sync(0xffffffffu, mine.x[q], owner);
+      t.y[q] = __shfl_sync(0xffffffffu, mine.y[q], owner);
+      t.sl[q] = __shfl_sync(0xffffffffu, mine.sl[q], owner);
+      t.idy[q] = __shfl_sync(0xffffffffu, mine.idy[q], owner);
+    }
+    t.scale = __shfl_sync(0xffffffffu, mine.scale, owner);
+    t.ox = __shfl_sync(0xffffffffu, mine.ox, owner);
+    t.oy = __shfl_sync(0xffffffffu, mine.oy, owner);
+    t.rlo = __shfl_sync(0xffffffffu, mine.rlo, owner);
+    t.map = __shfl_sync(0xffffffffu, mine.map, owner);
+    if (item < total) {
+      const DepositMaps& M = t.map == 0 ? m_total : (t.map == 1 ? m_min : m_sad);
+      deposit_row<D>(t, t.rlo + 1 + (item - before), npx, M);
+    }
+  }
 }
 
 // The 32 cells [base, base + 32) of an ncx-wide lattice whose corner rows are
-// vx apart (whole warp; lanes past ncells idle). For each half of the cells
-// (the triangles (y0, y1, y2), then (y2, y3, y0)): each lane classifies its
-// triangle (setup_head); a triangle inside one pixel deposits at once, lanes
-// in a row whose triangles fall in the same pixel adding once for all of
-// them; the others are prepared (setup_tail) and staged in shared memory,
-// compacted in lane order; the warp then scans their row counts and works
-// through the (triangle, row) items 32 at a time, each lane finding its
-// item's triangle by a binary search over the scan.
+// vx apart (whole warp; lanes past ncells idle).
 template <typename D>
 __device__ __forceinline__ void deposit_warp_cells(const double2* __restrict__ verts, long long ncx, long long vx,
                                                    long long ncells, long long base, D factor, int npx, int npy,
                                                    const DepositMaps& m_total, const DepositMaps& m_min,
-                                                   const DepositMaps& m_sad, int parities, TriStage<D>& stage,
+                                                   const DepositMaps& m_sad, int parities, TriSlots<D>& stage,
                                                    long long vstep = 1, double ox = 0.0, double oy = 0.0,
                                                    double inv_scale = 1.0) {
   const int lane = threadIdx.x & 31;
@@ -407,13 +442,23 @@ __device__ __forceinline__ void deposit_warp_cells(const double2* __restrict__ v
       y0.y *= inv_scale, y1.y *= inv_scale, y2.y *= inv_scale, y3.y *= inv_scale;
     }
   }
+  // each half's head: a triangle inside one pixel deposits at once, the
+  // others are staged in the warp's slots, compacted in lane order
+  // a cell whose four corners all lie beyond one edge of the map deposits
+  // nothing (setup_head would reject both its triangles)
+  const bool live =
+      c < ncells &&
+      !((y0.x >= npx && y1.x >= npx && y2.x >= npx && y3.x >= npx) || (y0.x <= 0 && y1.x <= 0 && y2.x <= 0 && y3.x <= 0) ||
+        (y0.y >= npy && y1.y >= npy && y2.y >= npy && y3.y >= npy) || (y0.y <= 0 && y1.y <= 0 && y2.y <= 0 && y3.y <= 0));
+  if (__ballot_sync(0xffffffffu, live) == 0u) return;
   const unsigned lt = (1u << lane) - 1u;
+  int n = 0;
 #pragma unroll 1
   for (int half = 0; half < 2; half++) {
     Tri<D> h;
     h.nrows = 0;  // idle lanes (past the last cell) deposit nothing
     h.single = 0;
-    if (c < ncells) {
+    if (live) {
       h = half == 0 ? setup_head<D>(y0.x, y0.y, y1.x, y1.y, y2.x, y2.y, factor, npx, npy, parities != 0)
                     : setup_head<D>(y2.x, y2.y, y3.x, y3.y, y0.x, y0.y, factor, npx, npy, parities != 0);
     }
@@ -428,46 +473,36 @@ __device__ __forceinline__ void deposit_warp_cells(const double2* __restrict__ v
       if (h.single && (starts >> lane & 1u)) {
         const unsigned later = starts & ~((2u << lane) - 1u);  // lane 31: mask of all bits, none later
         const int end = later ? __ffs(later) - 1 : 32;
-        red_add(a, (unsigned long long)(end - lane) * RN<D>::to_fix(RN<D>::mul(factor, D(kFixScale))));
+        atomicAdd(a, (unsigned long long)(end - lane) * RN<D>::to_fix(RN<D>::mul(factor, D(kFixScale))));
       }
     }
-    const bool rows = h.nrows > 0 && !h.single;
-    const unsigned b = __ballot_sync(0xffffffffu, rows);
-    if (b == 0u) continue;
-    const int slot = __popc(b & lt);
-    if (rows) {
-      setup_tail(h, factor);
-      stage.put(slot, h);
-    }
-    __syncwarp();
-    // inclusive scan of the staged triangles' row counts, lane s holding slot s
-    const int mycnt = lane < __popc(b) ? stage.nrows[lane] : 0;
-    int incl = mycnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int v = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += v;
-    }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    for (int it0 = 0; it0 < total; it0 += 32) {
-      const int item = it0 + lane;
-      int lo = 0, hi = 31;  // slot: first lane whose inclusive count exceeds item
-#pragma unroll
-      for (int step = 0; step < 5; step++) {
-        const int mid = (lo + hi) >> 1;
-        const int v = __shfl_sync(0xffffffffu, incl, mid);
-        if (v > item) hi = mid;
-        else lo = mid + 1;
-      }
-      const int before = __shfl_sync(0xffffffffu, incl - mycnt, lo);
-      if (item < total) deposit_row<D>(stage, lo, stage.rlo[lo] + (item - before), npx, m_total, m_min, m_sad);
-    }
-    __syncwarp();  // slots free for the next half
+    const bool cx = h.nrows > 0 && !h.single;
+    const unsigned b = __ballot_sync(0xffffffffu, cx);
+    if (cx) stage.put(n + __popc(b & lt), h);
+    n += __popc(b);
   }
+  __syncwarp();
+  // the staged ones go row by row, one per lane: one round when at most 32
+  // of the warp's 64 triangles need it (fine lattices), else two
+  for (int r0 = 0; r0 < n; r0 += 32) {
+    Tri<D> mine;
+    mine.nrows = 0;
+    if (r0 + lane < n) {
+      stage.get(r0 + lane, mine);
+      setup_tail(mine, factor);
+    }
+    deposit_rows_warp<D>(mine, npx, m_total, m_min, m_sad);
+  }
+  __syncwarp();  // slots free for the warp's next cells
 }
 
 // Cells of an ncx x ncy lattice whose (ncx+1) x (ncy+1) corner positions are in
-// `verts`, 32 consecutive cells per warp (deposit_warp_cells).
+// `verts`. A warp takes 32 consecutive cells; each lane classifies the two
+// triangles of its cell (setup_head); a triangle inside one pixel is
+// deposited at once; the others are staged in shared memory, compacted, and
+// then get their reciprocals and scale (setup_tail) and go row by row
+// (deposit_rows_warp), one per lane: one round when at most 32 of the warp's
+// 64 triangles need it (fine lattices), else two.
 template <typename D>
 __global__ void __launch_bounds__(kDepositWarps * 32, sizeof(D) == 4 ? 4 : 2)
     ipm_deposit_cells(const double2* __restrict__ verts, long long ncx, long long ncy, D factor, int npx, int npy,
@@ -475,8 +510,8 @@ __global__ void __launch_bounds__(kDepositWarps * 32, sizeof(D) == 4 ? 4 : 2)
   const long long ncells = ncx * ncy;
   const long long warp0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  __shared__ TriStage<D> stages[kDepositWarps];
-  TriStage<D>& stage = stages[threadIdx.x >> 5];
+  __shared__ TriSlots<D> slots[kDepositWarps];
+  TriSlots<D>& stage = slots[threadIdx.x >> 5];
   for (long long base = warp0 * 32; base < ncells; base += nwarps * 32)
     deposit_warp_cells<D>(verts, ncx, ncx + 1, ncells, base, factor, npx, npy, m_total, m_min, m_sad, parities, stage);
 }
@@ -506,8 +541,8 @@ __global__ void __launch_bounds__(kDepositWarps * 32, sizeof(D) == 4 ? 4 : 2)
                       long long diff_stride) {
   const long long warp0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  __shared__ TriStage<D> stages[kDepositWarps];
-  TriStage<D>& stage = stages[threadIdx.x >> 5];
+  __shared__ TriSlots<D> slots[kDepositWarps];
+  TriSlots<D>& stage = slots[threadIdx.x >> 5];
   for (long long g = warp0; g < nchunks; g += nwarps) {
     int lo = 0, hi = npieces - 1;  // last piece with chunk0 <= g
     while (lo < hi) {
@@ -520,14 +555,6 @@ __global__ void __launch_bounds__(kDepositWarps * 32, sizeof(D) == 4 ? 4 : 2)
     deposit_warp_cells<D>(verts + pc.voff, pc.ncx, pc.vstride, pc.ncx * pc.ncy, (g - pc.chunk0) * 32, pc.factor,
                           npx, npy, M, M, M, 0, stage, pc.vstep, pc.ox, pc.oy, pc.inv_scale);
   }
-}
-
-// Fixed point (modulo 2^64, read as signed) -> magnification: the rounding of
-// the pieces of a pixel's coverage can leave a few units below zero where its
-// true coverage is zero or nearly so; those read as 0.
-__device__ __forceinline__ double fix_to_double(unsigned long long v) {
-  const long long s = (long long)v;
-  return s > 0 ? double(s) * kFixInv : 0.0;
 }
 
 // Row prefix sum of the difference array added to the pieces: one warp per
@@ -585,7 +612,7 @@ __global__ void ipm_resolve_rows_out(int npx, int npy, DepositMaps m, T* __restr
           const long long k = (long long)y * npx + x + i;
           const unsigned long long v = m.acc[k] + (base + d[i]);
           m.acc[k] = v;
-          out[k] = T(fix_to_double(v));
+          out[k] = T(double(v) * kFixInv);
         }
       }
       carry += __shfl_sync(0xffffffffu, incl, 31);
@@ -602,11 +629,11 @@ __global__ void ipm_finalize(long long n, const unsigned long long* __restrict__
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
     if (parities) {
       unsigned long long a = acc_min[k], b = acc_sad[k];
-      out_min[k] = T(fix_to_double(a));
-      out_sad[k] = T(fix_to_double(b));
-      out_total[k] = T(fix_to_double(a + b));
+      out_min[k] = T(double(a) * kFixInv);
+      out_sad[k] = T(double(b) * kFixInv);
+      out_total[k] = T(double(a + b) * kFixInv);
     } else {
-      out_total[k] = T(fix_to_double(acc_total[k]));
+      out_total[k] = T(double(acc_total[k]) * kFixInv);
     }
   }
 }

@@ -975,7 +975,7 @@ void orc_ipm_deposit_ref(long long ncx, long long ncy, const double* vx, const d
 #define CAT(a, b) CAT2(a, b)
 #define FN(name) CAT(name, SUF)
 #define TRI(suf) CAT(Tri, suf)
-#define ADDS(suf) CAT(Adds, suf)
+#define STRIP(suf) CAT(Strip, suf)
 
 #define D float
 #define SUF f32
