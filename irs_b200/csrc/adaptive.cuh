@@ -58,7 +58,8 @@ struct LeafView {
 };
 
 __device__ __forceinline__ LeafView make_leaf_view(const ShootParams& sp, const float4* near, const float2* coef,
-                                                   int nn, double cx, double cy, double hl) {
+                                                   int nn, double cx, double cy, double hl,
+                                                   double2 smooth0 = make_double2(0.0, 0.0)) {
   LeafView L;
   L.near = near;
   L.coef = coef;
@@ -72,12 +73,15 @@ __device__ __forceinline__ LeafView make_leaf_view(const ShootParams& sp, const 
   L.scy = sp.npy / (2.0 * sp.hly_im);
   L.pcx = ((L.lin_x * cx - sp.cy_re) + sp.hly_re) * L.scx;
   L.pcy = ((L.lin_y * cy - sp.cy_im) + sp.hly_im) * L.scy;
+  L.pcx -= smooth0.x * L.scx;  // a folded smooth sheet's value at the leaf centre (else 0)
+  L.pcy -= smooth0.y * L.scy;
   return L;
 }
 
 __device__ __forceinline__ LeafView leaf_view(const ShootParams& sp, const LeafPtrs& lp, int leaf) {
   return make_leaf_view(sp, lp.near32 + (size_t)leaf * kMaxStarsDirect, lp.coef32 + (size_t)leaf * kMaxOrder,
-                        lp.nnear[leaf], lp.cx[leaf], lp.cy[leaf], lp.hl[leaf]);
+                        lp.nnear[leaf], lp.cx[leaf], lp.cy[leaf], lp.hl[leaf],
+                        lp.smooth0 ? lp.smooth0[leaf] : make_double2(0.0, 0.0));
 }
 
 // Source position (pixel units, row axis flipped) of the lattice point (x, y)
@@ -239,7 +243,9 @@ __global__ void __launch_bounds__(256) ada_refine_tiles(AdaGeom g, ShootParams s
       if (threadIdx.x < kMaxStarsDirect) s_near[threadIdx.x] = lp.near32[(size_t)leaf * kMaxStarsDirect + threadIdx.x];
       if (threadIdx.x >= 64 && threadIdx.x < 64 + kMaxOrder)
         s_coef[threadIdx.x - 64] = lp.coef32[(size_t)leaf * kMaxOrder + threadIdx.x - 64];
-      if (threadIdx.x == 0) s_view = make_leaf_view(sp, s_near, s_coef, lp.nnear[leaf], lp.cx[leaf], lp.cy[leaf], lp.hl[leaf]);
+      if (threadIdx.x == 0)
+        s_view = make_leaf_view(sp, s_near, s_coef, lp.nnear[leaf], lp.cx[leaf], lp.cy[leaf], lp.hl[leaf],
+                                lp.smooth0 ? lp.smooth0[leaf] : make_double2(0.0, 0.0));
     }
     __syncthreads();
     const LeafView* stage = leaf >= 0 ? &s_view : nullptr;

@@ -166,7 +166,7 @@ class AdaptiveIPM {
     nty = int((ncy + kAdaTile - 1) / kAdaTile);
     g_ = AdaGeom{sp_.base_x, sp_.base_y, sp_.rhs_x, sp_.rhs_y, ncx, ncy, ntx, nty, p.num_pixels_y.re,
                  p.num_pixels_y.im};
-    generic_ = !(p.approx && !p.rectangular);
+    generic_ = !(p.approx && !p.rectangular) && !base.smooth_folded();
     cells_base = ncx * ncy;
   }
 

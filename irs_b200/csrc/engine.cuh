@@ -159,6 +159,9 @@ class MapMaker {
     if (precision == kPrecisionFP32) return true;
     return sizeof(T) == 4;
   }
+  // The FP32 form folds an approximate rectangular smooth sheet into the
+  // leaves' expansions (leaves.cuh) instead of summing its series per point.
+  bool smooth_folded() const { return use_fp32() && prm.rectangular && prm.approx; }
 
   Pix* pixels() { return h_pix.p; }
   // host buffer of num_pixels_y2 x num_pixels_y1 values that the next run()
@@ -272,7 +275,9 @@ class MapMaker {
     }
     if (!compute_fmm<T>(fmm_, tree_, d_stars_.p, prm.expansion_order, stream_)) return false;
     launches += 2LL * (tree_.levels + 1) + std::max(0, tree_.levels - 1);
-    if (!build_leaves<T>(leaves_, tree_, fmm_, d_stars_.p, double(prm.theta_star), stream_)) return false;
+    const SmoothFold fold{smooth_folded() ? 1 : 0, double(prm.kappa_star), double(prm.corner.re),
+                          double(prm.corner.im), 0.318309886183790671537767526745028724, prm.taylor_smooth, nullptr};
+    if (!build_leaves<T>(leaves_, tree_, fmm_, d_stars_.p, double(prm.theta_star), stream_, fold)) return false;
     launches += 6;
     num_leaves = leaves_.n;
     if (!shoot()) return false;
@@ -554,6 +559,7 @@ class MapMaker {
     lp.rect = tiles_.rect.p;
     lp.tile_off = tiles_.tile_off.p;
     lp.table = tiles_.table.p;
+    lp.smooth0 = smooth_folded() ? leaves_.smooth0.p : nullptr;
     lp.nleaves = leaves_.n;
     return lp;
   }
@@ -583,7 +589,7 @@ class MapMaker {
     LeafPtrs lp = leaf_ptrs();
     int grid = shoot_grid(tiles_.total);
     const bool par = !VERT && prm.write_parities;
-    const bool generic = !(prm.approx && !prm.rectangular);
+    const bool generic = !(prm.approx && !prm.rectangular) && !smooth_folded();
     IRSB_CKR(cudaEventRecord(ev_lat0_, stream_));
     launches++;
     if (tiles_.total == 0) {

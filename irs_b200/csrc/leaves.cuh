@@ -17,10 +17,23 @@
 //   coef64[l][k] = k * c_k, k = 1..p       (slot k-1)
 //   coef32[l][k] = theta^2 (k+1) c_{k+1} / hl, k = 0..p-1: conj(alpha_local) =
 //                  sum_k coef32[k] dz^k with dz = (z - c) / hl
+//   smooth0[l]   = D(conj(c)) when the smooth sheet is folded (below)
+//
+// Folding the smooth sheet (rectangular field, approximate sheet, FP32 form):
+// there alpha_smooth(z) + kappa_star z is a polynomial D in conj(z) of degree
+// taylor_smooth + 1 (alpha_smooth.cuh:62-127, the series in conj(z)/corner).
+// Its Taylor coefficients about the leaf centre, in units of the leaf's half
+// length, F_k = e_k hl^k with D = sum_k e_k (conj(z) - conj(c))^k, come from
+// D at 32 points of the circle |z - c| = hl and a discrete Fourier transform
+// (FP64; terms of order 32 and above, below (hl / |corner|)^32 of D, are
+// dropped). F_0 goes to smooth0, conj(F_k) for k = 1..p-1 is added to
+// coef32[k]; the kernels then evaluate the sheet with the far field instead of
+// its series at every point.
 #pragma once
 #include "common.cuh"
 #include "devutil.cuh"
 #include "fmm.cuh"
+#include "smooth.cuh"
 #include "tree.cuh"
 
 namespace irsb {
@@ -54,6 +67,7 @@ constexpr int kTileY = 32;
 
 struct LeafSet {
   int n = 0;
+  DevVec<double2> smooth0;  // folded smooth sheet at the leaf centres (when folded)
   DevVec<int> flag;
   DevVec<long long> pos;
   DevVec<int> node;
@@ -112,6 +126,14 @@ __global__ void leaf_compact(int n, const int* __restrict__ dn, const int* __res
 }
 
 // One warp per leaf: gather the near field and the expansion coefficients.
+// The smooth sheet to fold into the FP32 leaf coefficients (on = 0: none).
+struct SmoothFold {
+  int on;
+  double kstar, corner_re, corner_im, inv_pi;
+  int taylor_smooth;
+  double2* smooth0;  // [nleaves] out
+};
+
 template <typename T>
 __global__ void leaf_build(int nleaves, const int* __restrict__ dn, int p, double theta,
                            const double* __restrict__ theta_r, const int* __restrict__ rid,
@@ -121,7 +143,7 @@ __global__ void leaf_build(int nleaves, const int* __restrict__ dn, int p, doubl
                            const int* __restrict__ n_nbr, const StarRec<T>* __restrict__ stars,
                            const double2* __restrict__ loc, double* lcx, double* lcy, double* lhl, int* nnear,
                            double4* near64, float4* near32, double2* coef64, float2* coef32, int* leaf_rid,
-                           int* dstat) {
+                           int* dstat, SmoothFold fold = SmoothFold{0, 0, 0, 0, 0, 0, nullptr}) {
   if (dn) nleaves = *dn;
   int lane = threadIdx.x & 31;
   int warps = (gridDim.x * blockDim.x) >> 5;
@@ -164,13 +186,39 @@ __global__ void leaf_build(int nleaves, const int* __restrict__ dn, int p, doubl
       near32[(size_t)l * kMaxStarsDirect + slot] = make_float4(0, 0, 0, 0);
     }
     if (lane == 0) nnear[l] = out;
+    // the folded smooth sheet: lane j samples D at the point j of the circle
+    // |z - c| = hl, then lane k forms F_k = (1/32) sum_j D_j e^{2 pi i j k / 32}
+    double2 fk = make_double2(0.0, 0.0);
+    if (fold.on) {
+      double sj, cj;
+      sincospi(double(lane) / 16.0, &sj, &cj);
+      const cplx<double> z = mk(ccx + h * cj, ccy + h * sj);
+      const cplx<double> a = alpha_smooth_(z, fold.kstar, 1, mk(fold.corner_re, fold.corner_im), 1,
+                                           fold.taylor_smooth, fold.inv_pi);
+      const double dre = a.re + fold.kstar * z.re, dim = a.im + fold.kstar * z.im;
+      for (int j = 0; j < 32; j++) {
+        const double xr = __shfl_sync(0xffffffffu, dre, j), xi = __shfl_sync(0xffffffffu, dim, j);
+        double sw, cw;
+        sincospi(double((j * lane) & 31) / 16.0, &sw, &cw);
+        fk.x += xr * cw - xi * sw;
+        fk.y += xr * sw + xi * cw;
+      }
+      fk.x *= 1.0 / 32.0;
+      fk.y *= 1.0 / 32.0;
+      if (lane == 0) fold.smooth0[l] = fk;
+    }
     // local expansion coefficients
     if (lane < p) {
       int kk = lane + 1;
       double2 c = loc[(size_t)k * (p + 1) + kk];
       if (coef64) coef64[(size_t)l * kMaxOrder + lane] = make_double2(c.x * kk, c.y * kk);
       double s = th2 * kk / h;
-      coef32[(size_t)l * kMaxOrder + lane] = make_float2(float(c.x * s), float(c.y * s));
+      double cr = c.x * s, ci = c.y * s;
+      if (fold.on && lane >= 1) {  // conj(F_k) into the coefficient of dz^k
+        cr += fk.x;
+        ci -= fk.y;
+      }
+      coef32[(size_t)l * kMaxOrder + lane] = make_float2(float(cr), float(ci));
     } else if (lane < kMaxOrder) {
       if (coef64) coef64[(size_t)l * kMaxOrder + lane] = make_double2(0, 0);
       coef32[(size_t)l * kMaxOrder + lane] = make_float2(0, 0);
@@ -256,7 +304,8 @@ __global__ void leaf_rects_batch(const int* __restrict__ dn, const int* __restri
 }
 
 template <typename T>
-bool build_leaves(LeafSet& L, TreeDev<T>& t, FmmDev& f, const StarRec<T>* stars, double theta, cudaStream_t s) {
+bool build_leaves(LeafSet& L, TreeDev<T>& t, FmmDev& f, const StarRec<T>* stars, double theta, cudaStream_t s,
+                  SmoothFold fold = SmoothFold{0, 0, 0, 0, 0, 0, nullptr}) {
   int n = t.num_nodes;
   if (!L.flag.alloc_exact(n) || !L.pos.alloc_exact(n + 1)) return false;
   int blocks = std::max(1, std::min(ceil_div(n, 256), 148 * 8));
@@ -271,13 +320,17 @@ bool build_leaves(LeafSet& L, TreeDev<T>& t, FmmDev& f, const StarRec<T>* stars,
       !L.near32.alloc_exact((size_t)L.n * kMaxStarsDirect) || !L.coef64.alloc_exact((size_t)L.n * kMaxOrder) ||
       !L.coef32.alloc_exact((size_t)L.n * kMaxOrder))
     return false;
+  if (fold.on) {
+    if (!L.smooth0.alloc_exact(L.n)) return false;
+    fold.smooth0 = L.smooth0.p;
+  }
   leaf_compact<<<blocks, 256, 0, s>>>(n, nullptr, L.flag.p, L.pos.p, L.node.p);
   IRSB_LAUNCH_CK("leaf_compact");
   IRSB_CKR(cudaMemsetAsync(t.dstat.p, 0, 2 * sizeof(int), s));
   int lb = std::max(1, std::min(ceil_div(L.n, 8), 148 * 16));
   leaf_build<T><<<lb, 256, 0, s>>>(L.n, nullptr, f.p, theta, nullptr, nullptr, L.node.p, t.cx.p, t.cy.p, t.hl.p, t.sbeg.p, t.scnt.p, t.nbr.p,
                                    t.n_nbr.p, stars, f.loc.p, L.cx.p, L.cy.p, L.hl.p, L.nnear.p, L.near64.p,
-                                   L.near32.p, L.coef64.p, L.coef32.p, nullptr, t.dstat.p);
+                                   L.near32.p, L.coef64.p, L.coef32.p, nullptr, t.dstat.p, fold);
   IRSB_LAUNCH_CK("leaf_build");
   int st = 0;
   IRSB_CKR(cudaMemcpyAsync(&st, t.dstat.p, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -66,6 +66,10 @@ struct LeafPtrs {
   const long long* tile_off;
   const int4* table;  // per tile: leaf, i0, j0, (ni << 16) | nj
   int nleaves;
+  // constant term, at the leaf centre, of the smooth sheet's deviation from
+  // -kappa_star z where that deviation is folded into coef32 (rectangular
+  // field, approximate sheet, FP32 form); nullptr: not folded
+  const double2* smooth0 = nullptr;
 };
 
 struct TileInfo {
@@ -277,8 +281,13 @@ __device__ __forceinline__ void shoot_f32_tile(const ShootParams& sp, const Leaf
     const double lcx = lp.cx[ti.leaf], lcy = lp.cy[ti.leaf];
     const float inv_hl = float(1.0 / lp.hl[ti.leaf]);
     // leaf-centre part of the source position, in pixel units
-    const double pcx = ((lin_x * lcx - sp.cy_re) + sp.hly_re) * scx;
-    const double pcy = ((lin_y * lcy - sp.cy_im) + sp.hly_im) * scy;
+    double pcx = ((lin_x * lcx - sp.cy_re) + sp.hly_re) * scx;
+    double pcy = ((lin_y * lcy - sp.cy_im) + sp.hly_im) * scy;
+    if (lp.smooth0) {  // the folded smooth sheet's value at the leaf centre
+      const double2 d0 = lp.smooth0[ti.leaf];
+      pcx -= d0.x * scx;
+      pcy -= d0.y * scy;
+    }
     __syncthreads();
     const int nn4 = (nn + 3) & ~3;
     if (tx < ti.ni) {
