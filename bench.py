@@ -563,6 +563,66 @@ def adaptive_measure():
     return res
 
 
+CONFIG3 = dict(kappa_tot=0.7, shear=0.2, smooth_fraction=0.1, theta_star=1.0, mass_function="kroupa", m_lower=0.01,
+               m_upper=1.5, rectangular=True, approx=True, half_length_y1=50.0, half_length_y2=50.0,
+               num_pixels_y1=8192, num_pixels_y2=8192, random_seed=3, expansion_order=16, write_histograms=0)
+
+
+def config3_measure():
+    """The rectangular Kroupa configuration: 8192^2 map, approximate smooth
+    sheet (degree-39 series), expansion order 16; IRS at 64 rays per pixel
+    (1.1e11 rays, 4.3e5 stars) and IPM at one cell per pixel (2.5e9 cells,
+    6.5e5 stars), FP32 form, device time of the whole pipeline (best of 2)."""
+    import irs_b200
+    out = {}
+    r = irs_b200.IRS(**CONFIG3, num_rays_y=64, is_double=False)
+    r.run()
+    ts = [r.rerun(1) for _ in range(2)]
+    t = float(np.min(ts))
+    out["irs"] = {"rays": int(r.num_rays_shot), "stars": int(r.num_stars), "rays_received": int(r.num_rays_received),
+                  "s_per_map": t, "lattice_s": r.value("t_lattice"), "rays_per_s": r.num_rays_shot / t}
+    r.close()
+    m = irs_b200.IPM(**CONFIG3, num_rays_y=1, is_double=False)
+    m.run()
+    ts = [m.rerun(1) for _ in range(2)]
+    t = float(np.min(ts))
+    out["ipm"] = {"cells": int(m.value("num_ray_threads_1") * m.value("num_ray_threads_2")), "stars": int(m.num_stars),
+                  "s_per_map": t, "lattice_ms": m.value("t_lattice") * 1e3, "deposit_ms": m.value("t_deposit") * 1e3,
+                  "pixels_per_s": 8192 * 8192 / t}
+    m.close()
+    return out
+
+
+def config3_errors(threads, n=4000):
+    """Config-3 IPM FP32 corner positions against the FP64 direct sum over all
+    stars: a seeded sample of corners of two cell rows through the lattice centre."""
+    import irs_b200
+    from oracle import pyoracle as po
+    from tests.cases import lattice, oracle_lens, to_pixels
+    m = irs_b200.IPM(**CONFIG3, num_rays_y=1, is_double=False)
+    m.derive()
+    ny = int(m.value("num_ray_threads_2"))
+    j0 = ny // 2
+    m.lib.set_band(m.obj, j0, j0 + 2)
+    m.run()
+    v = m.vertices()
+    rng = np.random.default_rng(0)
+    jj, ii = rng.integers(0, v.shape[0], n), rng.integers(0, v.shape[1], n)
+    x, _ = lattice(m, vertices=True)
+    oy = m.value("center_x2") - m.value("half_length_x2")
+    y = oy + 2.0 * (m.value("ray_half_sep_2") * (j0 + jj).astype(np.float64))
+    t0 = time.perf_counter()
+    wx, wy = po.shoot_direct(m.stars.astype(np.float64), oracle_lens(m), x[ii], y, threads=threads)
+    dt = time.perf_counter() - t0
+    px, py = to_pixels(m, wx, wy)
+    err = np.hypot(v[jj, ii, 0] - px, v[jj, ii, 1] - py)
+    nstars = int(m.num_stars)
+    m.close()
+    return {"sample": f"{n} random corners of cell rows {j0}..{j0 + 2} of {ny}, direct sum over all "
+                      f"{nstars} stars {dt:.1f} s",
+            "median_px": float(np.median(err)), "p99_px": float(np.quantile(err, 0.99)), "max_px": float(err.max())}
+
+
 CCF_CASES = (137, 1000, 4000)  # stars; kappa_tot 0.3, shear 0.3, kappa_star 0.27 (the reference CCF defaults)
 
 
@@ -787,7 +847,8 @@ def our_arm(args):
         tp = [plain.rerun(1) for _ in range(max(2, args.steps // 2))]
         extra["ipm_fp64_plain"] = {"pixels_per_s": npix / float(np.mean(tp)), "ms_per_step": float(np.mean(tp)) * 1e3,
                                    "lattice_ms": plain.value("t_lattice") * 1e3,
-                                   "deposit_ms": plain.value("t_deposit") * 1e3}
+                                   "deposit_ms": plain.value("t_deposit") * 1e3,
+                                   "tree_expansions_ms": (plain.value("t_pipeline") - plain.value("t_shoot")) * 1e3}
         extra["ipm_fp32_over_fp64"] = float(np.mean(tp)) / (dev_time / args.steps)
         plain.close()
         import irs_b200
@@ -816,6 +877,7 @@ def our_arm(args):
                                                                                   seeded.magnifications))}
         seeded.close()
         gb.close()
+        extra["config3"] = config3_measure()
         extra["batched_256"] = batch_measure(args.steps)
         extra["learned_adaptive"] = adaptive_measure()
         extra["ccf"] = ccf_measure()
@@ -827,6 +889,8 @@ def our_arm(args):
             if not args.no_extra:
                 cpu["ccf_reference"] = ccf_cpu_reference(extra.get("ccf"))
             errs["irs_case1"] = irs_case1_errors(os.cpu_count() or 1)
+            if not args.no_extra:
+                errs["config3_ipm_corners"] = config3_errors(os.cpu_count() or 1)
         out = {
             "metric": "IPM pixels/s", "value": value, "unit": "pixels/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_time / args.steps * 1e3, "higher_is_better": True,
