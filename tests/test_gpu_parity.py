@@ -7,6 +7,8 @@ Tolerances:
   * FP64 plain form: source positions within 1e-9 pixel of the oracle's FMM form
     (same expansion), IRS maps identical up to rays within rounding of a pixel
     edge (<= 2 rays);
+  * smooth sheets: the approximate (default) and the exact forms, circular and
+    rectangular fields, under the same bars;
   * FP32 form: source positions within 2e-3 pixel at the 99.9th percentile of
     the oracle's FMM form; IRS rays moved between pixels <= 1e-4 of those
     received; median relative magnification error vs the FP64 direct-sum
@@ -105,7 +107,10 @@ def _vertex_positions_oracle(m, t):
     return np.stack([px, py], -1).reshape(len(y), len(x), 2)
 
 
-@pytest.mark.parametrize("cfg", [IPM_SMALL, IPM_RECT], ids=["circle", "rect"])
+EXACT = [dict(IPM_SMALL, approx=False), dict(IPM_RECT, approx=False)]  # exact smooth sheets (alpha_smooth.cuh:62-127)
+
+
+@pytest.mark.parametrize("cfg", [IPM_SMALL, IPM_RECT] + EXACT, ids=["circle", "rect", "circle_exact", "rect_exact"])
 def test_ipm_fp64_vertices_match_oracle(gpu, cfg):
     m = _run(irs_b200.IPM, cfg, True, expansion_order=12)
     t = _oracle_tree(m)
@@ -116,7 +121,7 @@ def test_ipm_fp64_vertices_match_oracle(gpu, cfg):
     assert np.nanmax(err) < 1e-8
 
 
-@pytest.mark.parametrize("cfg", [IPM_SMALL, IPM_RECT], ids=["circle", "rect"])
+@pytest.mark.parametrize("cfg", [IPM_SMALL, IPM_RECT] + EXACT, ids=["circle", "rect", "circle_exact", "rect_exact"])
 def test_ipm_fp32_vertices_close_to_oracle(gpu, cfg):
     m = _run(irs_b200.IPM, cfg, False, expansion_order=12)
     t = _oracle_tree(m)
@@ -182,8 +187,9 @@ def _irs_oracle_map(m, t, want_mu=False):
     return po.irs_bin(wx, wy, m.center, m.half_length, m.num_pixels, mu=mu)
 
 
-def test_irs_fp64_matches_oracle(gpu):
-    m = _run(irs_b200.IRS, IRS_SMALL, True, expansion_order=10)
+@pytest.mark.parametrize("approx", [True, False], ids=["approx_sheet", "exact_sheet"])
+def test_irs_fp64_matches_oracle(gpu, approx):
+    m = _run(irs_b200.IRS, dict(IRS_SMALL, approx=approx), True, expansion_order=10)
     t = _oracle_tree(m)
     ref = _irs_oracle_map(m, t)
     got = m.magnifications

@@ -234,3 +234,83 @@ def test_unchanged_reference_wrapper_over_this_library(gpu, tmp_path):
         np.testing.assert_array_equal(z[f"mu{int(dbl)}"], m.magnifications)
         np.testing.assert_array_equal(z[f"st{int(dbl)}"], m.stars)
         m.close()
+
+
+def _star_field(shape, rng):
+    """A field that covers the starfile test lens's shooting region (kappa
+    0.45, shear 0.4, light_loss 0.01, half length 2): equal masses, uniform
+    in a disc of radius 56 (706 stars) or a rectangle of corner (11, 53) (167
+    stars), i.e. kappa_star ~0.225."""
+    if shape == "circle":
+        n, rad = 706, 56.0
+        r = rad * np.sqrt(rng.random(n))
+        a = 2 * np.pi * rng.random(n)
+        xy = np.stack([r * np.cos(a), r * np.sin(a)], 1)
+        corner = (rad, 0.0)
+    else:
+        n, corner = 167, (11.0, 53.0)
+        xy = (rng.random((n, 2)) * 2 - 1) * np.array(corner)
+    return np.concatenate([xy, np.ones((n, 1))], 1), corner
+
+
+@needs_ref
+@pytest.mark.parametrize("fmt", ["txt", "bin_float", "bin_double"])
+@pytest.mark.parametrize("shape", ["circle", "rect"])
+def test_starfile_ingest_matches_reference(gpu, tmp_path, fmt, shape):
+    """Star files (star.cuh:175-434): .txt (positions in units of the Einstein
+    radius, the field's shape from its moment of inertia, theta 1) and .bin in
+    float or double (told apart by the file size), through the reference's
+    IPM and this build's on the same map: identical parameters, stars and maps
+    (double builds)."""
+    rng = np.random.default_rng(42)
+    stars, corner = _star_field(shape, rng)
+    if fmt == "txt":
+        sf = str(tmp_path / "stars.txt")
+        np.savetxt(sf, stars, fmt="%.17g")
+    else:
+        sf = str(tmp_path / "stars.bin")
+        rg.write_starfile(sf, stars, shape == "rect", corner, 1.0, double=(fmt == "bin_double"))
+    p = dict(kappa_tot=0.45, shear=0.4, light_loss=0.01, safety_scale=1.1, starfile=sf, half_length_y1=2.0,
+             half_length_y2=2.0, num_pixels_y1=64, num_pixels_y2=64, num_rays_y=4, write_stars=1, write_maps=0,
+             write_histograms=0)
+    rd = tmp_path / "ref"
+    rd.mkdir()
+    r = rg.run_ipm(p, is_double=True, outdir=str(rd))
+    m = irs_b200.IPM(**p, is_double=True, outfile_prefix=str(tmp_path / "ours_"))
+    m.run()
+    m.save()
+    ours = rg.read_param_info(str(tmp_path / "ours_ipm_parameter_info.txt"))
+    for k, v in r["param_info"].items():
+        if k in SKIP_KEYS or isinstance(v, str):
+            continue
+        assert ours.get(k) == v, (k, ours.get(k), v)
+    np.testing.assert_array_equal(_sorted(r["stars"]), _sorted(m.stars))
+    med, p99, mx = rel_err(m.magnifications, r["magnifications"])
+    assert med <= 1e-8 and p99 <= 1e-7, (med, p99, mx)
+    m.close()
+
+
+@needs_ref
+def test_histograms_match_reference(gpu, tmp_path):
+    """The histogram files (ipm.cuh:950-1120, array_functions.cuh:114-160,
+    write_histogram :318-349): magnification x 1000 and log10 magnification x
+    1000, rounded, as (value, count) pairs, from the same star field (double
+    builds, whose maps agree to ~1e-10): the same bins, counts equal but for
+    pixels whose value sits within rounding of a bin edge (at most 2 per bin)."""
+    p = dict(headline_params(), half_length_y1=4.0, half_length_y2=4.0, num_pixels_y1=256, num_pixels_y2=256,
+             write_stars=0, write_maps=0, write_histograms=1)
+    rd = tmp_path / "ref"
+    rd.mkdir()
+    rg.run_ipm(p, is_double=True, outdir=str(rd))
+    m = irs_b200.IPM(**p, is_double=True, outfile_prefix=str(tmp_path / "ours_"))
+    m.run()
+    m.save()
+    for f in ("ipm_mags_numpixels.txt", "ipm_log_mags_numpixels.txt"):
+        a = np.loadtxt(rd / f, dtype=np.int64).reshape(-1, 2)
+        b = np.loadtxt(tmp_path / ("ours_" + f), dtype=np.int64).reshape(-1, 2)
+        assert a[:, 1].sum() == b[:, 1].sum() == 256 * 256
+        da, db = dict(map(tuple, a)), dict(map(tuple, b))
+        for k in set(da) | set(db):
+            assert abs(da.get(k, 0) - db.get(k, 0)) <= 2, (f, k, da.get(k), db.get(k))
+        assert sum(abs(da.get(k, 0) - db.get(k, 0)) for k in set(da) | set(db)) <= 8, f
+    m.close()

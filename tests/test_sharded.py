@@ -84,3 +84,38 @@ def test_gpu_bands_sum_to_full_map(gpu, kind):
         np.testing.assert_array_equal(acc, full.fixed_maps())
     else:
         np.testing.assert_array_equal(acc, full.magnifications)
+
+
+def _sharded_worker(rank, world, port, kind, out):
+    import torch.distributed as dist
+
+    import irs_b200
+    from irs_b200.sharded import sharded_run
+    from tests.cases import IPM_SMALL, IRS_SMALL
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    cls, cfg = (irs_b200.IPM, IPM_SMALL) if kind == "ipm" else (irs_b200.IRS, IRS_SMALL)
+    m = cls(**cfg, expansion_order=10)
+    total, _, _ = sharded_run(m)
+    if rank == 0:
+        np.save(out, total)
+    m.close()
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["ipm", "irs"])
+def test_sharded_run_two_gloo_ranks_on_one_gpu(gpu, tmp_path, kind):
+    """The product's sharded_run with two ranks (processes) sharing cuda:0,
+    each shooting its band, reduced over gloo: the same map as one object."""
+    import irs_b200
+    from tests.cases import IPM_SMALL, IRS_SMALL
+    out = str(tmp_path / "map.npy")
+    mp.spawn(_sharded_worker, args=(2, _free_port(), kind, out), nprocs=2, join=True)
+    cls, cfg = (irs_b200.IPM, IPM_SMALL) if kind == "ipm" else (irs_b200.IRS, IRS_SMALL)
+    full = cls(**cfg, expansion_order=10)
+    full.run()
+    np.testing.assert_array_equal(np.load(out), full.magnifications)
+    full.close()
