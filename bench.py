@@ -238,10 +238,12 @@ def cpu_baseline(m, stars, threads, budget_s=12.0):
     got = po.ipm_deposit_fixed(v[j0:j0 + rows + 1], factor32, m.num_pixels, single=True).astype(np.float64)
     ok = ref > 0
     rel = np.abs(got[ok] - ref[ok]) / ref[ok]
+    big = ref[ok] >= 0.1 * ref[ok].mean()  # pixels the band covers substantially
     chk["band_map"] = {"sample": f"cell rows {j0}..{j0 + rows} of {ny} (all {nx} columns, {rows * nx} cells, "
                                  f"{int(ok.sum())} pixels touched), direct sum {t_band:.1f} s",
                        "median_rel": float(np.median(rel)), "p99_rel": float(np.quantile(rel, 0.99)),
                        "max_rel": float(rel.max()),
+                       "max_rel_covered": float(rel[big].max()), "covered_pixels": int(big.sum()),
                        "flux_weighted_rel": float(np.abs(got - ref).sum() / ref.sum())}
     return out, chk
 
@@ -926,11 +928,34 @@ def main():
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
     ap.add_argument("--size", default="full", choices=["full", "small"],
                     help="small: 500 x 500 map at the same pixel scale (for profiler captures)")
+    ap.add_argument("--case", default=None, choices=["config3-irs-band"],
+                    help="profiler capture of one case: config3-irs-band = the rectangular Kroupa IRS configuration "
+                         "(order 16, 64 rays per pixel) on 512 ray rows through the lattice centre, --steps runs")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.case:
+        profile_case(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         our_arm(args)
+
+
+def profile_case(args):
+    """A small case for profiler captures (not a bench line): prints the
+    device time per run of the IRS lens-equation kernel."""
+    import irs_b200
+    r = irs_b200.IRS(**CONFIG3, num_rays_y=64, is_double=False)
+    r.derive()
+    ny = int(r.value("num_ray_threads_2"))
+    r.lib.set_band(r.obj, ny // 2 - 256, ny // 2 + 256)
+    r.run()
+    ts = []
+    for _ in range(max(1, args.steps)):
+        r.rerun(1)
+        ts.append(r.value("t_lattice"))
+    print(json.dumps({"case": args.case, "rays": int(r.num_rays_shot), "lattice_ms": float(np.min(ts)) * 1e3,
+                      "rays_per_s": r.num_rays_shot / float(np.min(ts))}))
+    r.close()
 
 
 if __name__ == "__main__":
