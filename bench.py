@@ -15,10 +15,16 @@ step, IPM.run() copies the star field from host memory, runs the full pipeline
 (including the histograms) and returns the map as a numpy array in host memory
 (IPM.magnifications), timed on the host clock.
 
+Both arms use one star field (workload_stars: numpy PCG64, the workload's
+seed), handed to this build through set_stars.
+
 --impl reference times the reference's own IPM on the host CPU cores (its tree,
 expansions and cell-shooting kernel compiled for the host, OpenMP; the oracle's
-restatement where that library was not built), the tree once per step and a
-band of cell rows scaled to the full lattice.
+restatement where that library was not built): each step a band of cell rows
+plus the band's share of the tree's time (built once), the pixels accounted
+being the band's share of the map; the whole map once beside it, and the
+reference's own GPU build on the same star field (secondary.reference_gpu).
+No library of this build is loaded by that arm.
 Under torchrun every rank runs an independent replica (the map of one
 realisation is not sharded here); value sums the replicas.
 """
