@@ -180,6 +180,7 @@ void ada_set_error_mode(void* ada, int mode);   /* error as a share of 0: the ti
 void ada_set_quantile(void* ada, float q);                        /* network: smallest level with cumulative p >= q */
 void ada_set_max_level(void* ada, int level);                     /* labels / network stop here; the audit may go to 16 */
 void ada_set_audit(void* ada, double fraction, unsigned seed);
+void ada_set_audit_bound(void* ada, double bound);             /* audited miss share above which the level choice escalates */
 void ada_set_refine_capacity(void* ada, long long corners);       /* refinement buffer, 0: automatic */
 void ada_set_tiled_min(void* ada, int tiles);  /* chunks of >= tiles use the tiled lens kernel, smaller point by point */
 void ada_set_network(void* ada, const float* w, const float* mu, const float* sig); /* 5061 weights, 8 + 8 */

@@ -50,7 +50,7 @@ IPM_ONLY_SYMBOLS = ["ipm_deposit_noalloc", "batch_init", "batch_destroy", "batch
                     "batch_copy_maps", "batch_maps_device", "batch_copy_stars", "batch_get_value",
                     "ada_init", "ada_destroy", "ada_base", "ada_set_policy", "ada_set_levels", "ada_set_tolerance", "ada_set_quantile", "ada_set_error_mode",
                     "ada_set_max_level",
-                    "ada_set_audit", "ada_set_refine_capacity", "ada_set_tiled_min", "ada_set_network", "ada_run", "ada_num_tiles",
+                    "ada_set_audit", "ada_set_audit_bound", "ada_set_refine_capacity", "ada_set_tiled_min", "ada_set_network", "ada_run", "ada_num_tiles",
                     "ada_copy_features", "ada_copy_levels", "ada_labels", "ada_copy_map", "ada_get_value",
                     "mlp_num_params", "mlp_train", "mlp_gradients", "mlp_predict"]
 
@@ -192,7 +192,7 @@ def _bind(lib, kind: str, is_double: bool):
                 ("ada_set_policy", [vp, C.c_int, C.c_int], None), ("ada_set_levels", [vp, ip, C.c_int], None),
                 ("ada_set_tolerance", [vp, C.c_double], None), ("ada_set_quantile", [vp, C.c_float], None),
                 ("ada_set_error_mode", [vp, C.c_int], None), ("ada_set_max_level", [vp, C.c_int], None),
-                ("ada_set_audit", [vp, C.c_double, C.c_uint], None),
+                ("ada_set_audit", [vp, C.c_double, C.c_uint], None), ("ada_set_audit_bound", [vp, C.c_double], None),
                 ("ada_set_refine_capacity", [vp, C.c_longlong], None), ("ada_set_tiled_min", [vp, C.c_int], None), ("ada_set_network", [vp, fp, fp, fp], None),
                 ("ada_run", [vp, C.c_int], C.c_bool), ("ada_num_tiles", [vp], C.c_int),
                 ("ada_copy_features", [vp, fp], C.c_bool), ("ada_copy_levels", [vp, ip, C.c_int], C.c_bool),

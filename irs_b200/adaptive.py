@@ -93,12 +93,17 @@ class AdaptiveIPM:
     tile's own flux (error_mode 0) or of the map's flux where the tile lands
     (error_mode 1). max_level: the largest level of labels and network
     choices (tiles near stars would ask for 16 at a large cost and a small
-    gain in the map); the audit still sends a failing tile to 16. quantile: a tile takes the smallest level whose cumulative network
+    gain in the map); the audit still sends a failing tile to 16.
+    audit_bound: when more than this share of the audited tiles misses the
+    tolerance at its chosen level, the choice escalates (network quantiles
+    0.9, 0.95, 0.99, then every tile one level finer up to max_level).
+    quantile: a tile takes the smallest level whose cumulative network
     probability reaches it (above 0.5 leans towards refining). The map inputs
     are those of IPM (keyword arguments)."""
 
-    def __init__(self, network=None, policy="network", level=1, levels=None, tolerance=1e-4,
-                 audit_fraction=0.01, audit_seed=1, refine_capacity=0, quantile=0.8, error_mode=0, max_level=8,
+    def __init__(self, network=None, policy="network", level=1, levels=None, tolerance=1e-3,
+                 audit_fraction=0.01, audit_seed=1, audit_bound=0.05, refine_capacity=0, quantile=0.8, error_mode=0,
+                 max_level=8,
                  tiled_min=1 << 30, is_double=False,
                  verbose=0,
                  **ipm_kwargs):
@@ -126,6 +131,7 @@ class AdaptiveIPM:
         self.lib.ada_set_max_level(self.h, int(max_level))
         self.lib.ada_set_tiled_min(self.h, int(tiled_min))
         self.lib.ada_set_audit(self.h, float(audit_fraction), int(audit_seed))
+        self.lib.ada_set_audit_bound(self.h, float(audit_bound))
         self.lib.ada_set_refine_capacity(self.h, int(refine_capacity))
 
     def close(self):

@@ -34,7 +34,7 @@ class AdaptiveIPM {
   int policy = kAdaNetwork;
   int uniform_level = 1;
   std::vector<int> given_levels;
-  double eps = 1e-4;             // tolerance of a tile's deposit error (err_mode)
+  double eps = 1e-3;             // tolerance of a tile's deposit error (err_mode)
   int max_level = 8;  // labels and network choices stop here; only the audit sends tiles to 16
   int err_mode = 0;  // 0: share of the tile's own flux; 1: of the map's flux where it lands; 2: the smaller (ada_window_errors)
   double audit_fraction = 0.01;  // share of tiles audited per run
@@ -46,12 +46,21 @@ class AdaptiveIPM {
   int tiled_min = 1 << 30;
   std::vector<float> net_w, net_mu, net_sig;  // FP32 master weights, feature standardisation
   float net_quantile = 0.8f;  // a tile takes the smallest level whose cumulative probability reaches this
+  // audit bound: when more than this share of the audited tiles misses eps at
+  // its chosen level, the choice escalates (network quantiles 0.9, 0.95,
+  // 0.99, then every tile one level finer, up to max_level) to the first
+  // choice whose audited share is within the bound; audited tiles that still
+  // miss go to level 16
+  double fail_bound = 0.05;
 
   // results
   int ntx = 0, nty = 0;
   std::vector<int> level, predicted;  // per tile, subdivision 1..16
   long long cells_base = 0, cells_evaluated = 0, audit_cells = 0;
   int audited = 0, audit_failures = 0;
+  double fail_rate_initial = 0, fail_rate = 0;  // audited share missing eps: the network's choice, the final choice
+  int escalation = 0;  // 0: none; 1-3: network quantile 0.9 / 0.95 / 0.99; 4+: 3 + levels raised
+  float quantile_used = 0.8f;
   double t_base = 0, t_adapt = 0;                          // seconds
   double t_select = 0, t_audit = 0, t_refine_deposit = 0;  // parts of t_adapt
 
@@ -222,14 +231,8 @@ class AdaptiveIPM {
       IRSB_CKR(cudaMemcpyAsync(d_mu_.p, net_mu.data(), kMlpIn * sizeof(float), cudaMemcpyHostToDevice, s));
       IRSB_CKR(cudaMemcpyAsync(d_sig_.p, net_sig.data(), kMlpIn * sizeof(float), cudaMemcpyHostToDevice, s));
       mlp_to_bf16<<<ceil_div(kMlpParams, 256), 256, 0, s>>>(d_wf_.p, d_w_.p);
-      mlp_classify<<<std::max(1, std::min(ceil_div(nt, 128), 148 * 4)), 128, 0, s>>>(d_w_.p, d_mu_.p, d_sig_.p,
-                                                                                     d_feat_.p, nt, net_quantile,
-                                                                                     d_cls_.p);
-      IRSB_LAUNCH_CK("mlp_classify");
-      std::vector<int> cls(nt);
-      IRSB_CKR(cudaMemcpyAsync(cls.data(), d_cls_.p, nt * sizeof(int), cudaMemcpyDeviceToHost, s));
-      IRSB_CKR(cudaStreamSynchronize(s));
-      for (int t = 0; t < nt; t++) level[t] = std::min(ada_level_of(cls[t]), std::max(1, max_level));
+      if (!classify(net_quantile, level)) return false;
+      quantile_used = net_quantile;
     }
     for (int v : level)
       if (v != 1 && v != 2 && v != 4 && v != 8 && v != 16) {
@@ -237,6 +240,21 @@ class AdaptiveIPM {
         return false;
       }
     predicted = level;
+    return true;
+  }
+
+  // The network's levels of all tiles at cumulative-probability quantile q.
+  bool classify(float q, std::vector<int>& lv) {
+    const int nt = num_tiles();
+    cudaStream_t s = base.stream_;
+    mlp_classify<<<std::max(1, std::min(ceil_div(nt, 128), 148 * 4)), 128, 0, s>>>(d_w_.p, d_mu_.p, d_sig_.p,
+                                                                                   d_feat_.p, nt, q, d_cls_.p);
+    IRSB_LAUNCH_CK("mlp_classify");
+    std::vector<int> cls(nt);
+    IRSB_CKR(cudaMemcpyAsync(cls.data(), d_cls_.p, nt * sizeof(int), cudaMemcpyDeviceToHost, s));
+    IRSB_CKR(cudaStreamSynchronize(s));
+    lv.resize(nt);
+    for (int t = 0; t < nt; t++) lv[t] = std::min(ada_level_of(cls[t]), std::max(1, max_level));
     return true;
   }
 
@@ -356,6 +374,40 @@ class AdaptiveIPM {
     std::vector<float> err(tiles.size() * 4);
     if (!fine_errors(tiles, err)) return false;
     audited = int(tiles.size());
+    // share of the audited tiles that a level assignment leaves above eps
+    auto miss_rate = [&](const std::vector<int>& lv) {
+      int miss = 0;
+      for (size_t k = 0; k < tiles.size(); k++) {
+        const int c = __builtin_ctz(lv[tiles[k]]);
+        if (c < 4 && err[k * 4 + c] > eps) miss++;
+      }
+      return double(miss) / double(tiles.size());
+    };
+    fail_rate_initial = fail_rate = miss_rate(level);
+    escalation = 0;
+    if (policy == kAdaNetwork && fail_rate > fail_bound) {
+      const float qs[3] = {0.9f, 0.95f, 0.99f};
+      std::vector<int> lv;
+      for (int e = 0; e < 3 && fail_rate > fail_bound; e++) {
+        if (qs[e] <= quantile_used) continue;
+        if (!classify(qs[e], lv)) return false;
+        const double r = miss_rate(lv);
+        if (r < fail_rate || r <= fail_bound) {
+          level = lv, fail_rate = r, escalation = e + 1, quantile_used = qs[e];
+        }
+      }
+      for (int up = 1; fail_rate > fail_bound && up <= 4; up++) {  // every tile finer, capped at max_level
+        lv = level;
+        bool changed = false;
+        for (int& v : lv) {
+          const int w = std::min(v * 2, std::max(1, max_level));
+          changed = changed || w != v;
+          v = w;
+        }
+        if (!changed) break;
+        level = lv, fail_rate = miss_rate(lv), escalation = 3 + up;
+      }
+    }
     for (size_t k = 0; k < tiles.size(); k++) {
       const int t = tiles[k];
       audit_cells += (long long)tile_cells_x(t) * tile_cells_y(t) * kAdaMaxLevel * kAdaMaxLevel;

@@ -397,6 +397,7 @@ void ada_set_audit(void* a, double fraction, unsigned seed) {
   static_cast<Ada*>(a)->audit_fraction = fraction;
   static_cast<Ada*>(a)->audit_seed = seed;
 }
+void ada_set_audit_bound(void* a, double bound) { static_cast<Ada*>(a)->fail_bound = bound; }
 void ada_set_refine_capacity(void* a, long long n) { static_cast<Ada*>(a)->refine_cap = n; }
 void ada_set_tiled_min(void* a, int n) { static_cast<Ada*>(a)->tiled_min = n; }
 void ada_set_network(void* a, const float* w, const float* mu, const float* sig) {
@@ -433,6 +434,11 @@ double ada_get_value(void* a, const char* name) {
   if (n == "audit_cells") return double(ad->audit_cells);
   if (n == "audited") return ad->audited;
   if (n == "audit_failures") return ad->audit_failures;
+  if (n == "fail_rate_initial") return ad->fail_rate_initial;
+  if (n == "fail_rate") return ad->fail_rate;
+  if (n == "fail_bound") return ad->fail_bound;
+  if (n == "escalation") return ad->escalation;
+  if (n == "quantile_used") return ad->quantile_used;
   if (n == "t_base") return ad->t_base;
   if (n == "t_adapt") return ad->t_adapt;
   if (n == "t_select") return ad->t_select;

@@ -149,7 +149,7 @@ def test_network_gain_over_uniform_subdivision(gpu):
     def med(mu):
         return np.median(np.abs(mu[ok] - ref[ok]) / ref[ok])
 
-    a = run(policy="network", network=net, audit_fraction=0.05)
+    a = run(policy="network", network=net, audit_fraction=0.05, audit_bound=1.0)  # the network's own choice
     e_net = med(a.magnifications)
     base = a.value("cells_base")
     match = 16
@@ -162,3 +162,20 @@ def test_network_gain_over_uniform_subdivision(gpu):
           f"audit {a.value('audit_failures'):.0f}/{a.value('audited'):.0f}")
     assert e_net < 1e-3
     assert gain > 1.2
+
+
+def test_audit_escalates_above_the_bound(gpu):
+    """When more of the audited tiles miss the tolerance than the bound allows,
+    the level choice escalates (network quantile, then every tile finer): the
+    final miss share is not above the network's and levels only grow; with a
+    bound of 1 nothing escalates."""
+    net = LevelNet.load()
+    kw = dict(policy="network", network=net, audit_fraction=0.2, tolerance=EPS)
+    a = _ada(**kw, audit_bound=1.0)
+    b = _ada(**kw, audit_bound=0.0)
+    assert a.value("escalation") == 0 and a.value("fail_rate") == a.value("fail_rate_initial")
+    assert b.value("fail_rate_initial") == a.value("fail_rate_initial")
+    if a.value("fail_rate_initial") > 0:
+        assert b.value("escalation") > 0
+        assert b.value("fail_rate") <= b.value("fail_rate_initial")
+        assert np.all(b.levels() >= a.levels(predicted=True))
