@@ -504,12 +504,26 @@ def adaptive_measure():
         return float(np.median(r)), float(np.quantile(r, 0.99))
 
     cfg = ADAPTIVE_CONFIG
-    u16 = irs_b200.AdaptiveIPM(policy="uniform", level=16, audit_fraction=0.0, **cfg)
+    # one star field for every map below (the library's own draw for the
+    # configuration's seed, as the FP32 form stores it): a plain run at
+    # another num_rays_y would otherwise derive another star count
+    g = irs_b200.IPM(**cfg, is_double=False)
+    g.run()
+    field = (g.stars.astype(np.float64), (float(g.value("rad")), 0.0))
+    g.close()
+
+    def with_field(m):
+        base = m.base if hasattr(m, "base") else m
+        base.set_stars(field[0], rectangular=False, corner=field[1], theta_star=cfg["theta_star"])
+        base.safety_scale = SAFETY
+        return m
+
+    u16 = with_field(irs_b200.AdaptiveIPM(policy="uniform", level=16, audit_fraction=0.0, **cfg))
     u16.run()
     ref = u16.magnifications.astype(np.float64)
     u16_ms = (u16.value("t_base") + u16.value("t_adapt")) * 1e3
     u16.close()
-    a = irs_b200.AdaptiveIPM(tolerance=1e-3, audit_fraction=0.0025, audit_bound=0.05, **cfg)
+    a = with_field(irs_b200.AdaptiveIPM(tolerance=1e-3, audit_fraction=0.0025, audit_bound=0.05, **cfg))
     a.run()  # warm-up
     runs = []
     for _ in range(3):  # the best of three warm runs (one seed: the same map each time)
@@ -532,13 +546,13 @@ def adaptive_measure():
     med_a, p99_a = rel_err(mu_a, ref)
     res.update({"median_rel_err_vs_uniform16": med_a, "p99_rel_err_vs_uniform16": p99_a})
     for L in (1, 2, 4, 8):
-        u = irs_b200.AdaptiveIPM(policy="uniform", level=L, audit_fraction=0.0, **cfg)
+        u = with_field(irs_b200.AdaptiveIPM(policy="uniform", level=L, audit_fraction=0.0, **cfg))
         u.run()
         res[f"uniform{L}_median_rel_err"] = rel_err(u.magnifications, ref)[0]
         u.close()
     # the plain uniform FP64 form at level 8 (num_rays_y = 64) over its whole lattice
     L = 8
-    p = irs_b200.IPM(**{**cfg, "num_rays_y": L * L}, is_double=True)
+    p = with_field(irs_b200.IPM(**{**cfg, "num_rays_y": L * L}, is_double=True))
     p.derive()
     ny, nx = int(p.value("num_ray_threads_2")), int(p.value("num_ray_threads_1"))
     rows = max(1, int(2.5e8 // (nx + 1)))  # corner buffer of a band: 4 GB at most
