@@ -944,9 +944,10 @@ def main():
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
     ap.add_argument("--size", default="full", choices=["full", "small"],
                     help="small: 500 x 500 map at the same pixel scale (for profiler captures)")
-    ap.add_argument("--case", default=None, choices=["config3-irs-band"],
+    ap.add_argument("--case", default=None, choices=["config3-irs-band", "adaptive"],
                     help="profiler capture of one case: config3-irs-band = the rectangular Kroupa IRS configuration "
-                         "(order 16, 64 rays per pixel) on 512 ray rows through the lattice centre, --steps runs")
+                         "(order 16, 64 rays per pixel) on 512 ray rows through the lattice centre, --steps runs; "
+                         "adaptive = the learned-adaptive map (4096^2), --steps runs")
     args = ap.parse_args()
     if args.case:
         profile_case(args)
@@ -958,8 +959,18 @@ def main():
 
 def profile_case(args):
     """A small case for profiler captures (not a bench line): prints the
-    device time per run of the IRS lens-equation kernel."""
+    device time per run of the IRS lens-equation kernel, or of the adaptive
+    map's base and adaptive passes."""
     import irs_b200
+    if args.case == "adaptive":
+        a = irs_b200.AdaptiveIPM(tolerance=1e-3, audit_fraction=0.0025, audit_bound=0.05, **ADAPTIVE_CONFIG)
+        for _ in range(max(1, args.steps)):
+            a.run()
+        print(json.dumps({"case": args.case, "t_base_ms": a.value("t_base") * 1e3, "t_adapt_ms": a.value("t_adapt") * 1e3,
+                          "t_refine_deposit_ms": a.value("t_refine_deposit") * 1e3,
+                          "cells_evaluated": a.value("cells_evaluated")}))
+        a.close()
+        return
     r = irs_b200.IRS(**CONFIG3, num_rays_y=64, is_double=False)
     r.derive()
     ny = int(r.value("num_ray_threads_2"))
