@@ -137,10 +137,13 @@ bool copy_fixed_maps(IPMHandle* self, unsigned long long* total, unsigned long l
  * (ncx+1) x (ncy+1) corner source positions at the device pointer verts
  * (double x, y pixel units, row axis flipped) into the npx x npy map at the
  * device pointer map, on the given cudaStream_t (NULL: default stream),
- * asynchronously. Scratch is a static device array: maps up to 1024 x 1024
- * pixels; larger sizes return 1. Its first call on a device looks up the
- * array's device address (make it before any stream capture); calls that
- * overlap on the GPU race on the shared scratch. Returns 0 on success. */
+ * asynchronously. Scratch is one static device array per GPU (16.8 MB): maps
+ * of at most 1024 * 1024 pixels in all and at most 1024 rows; larger sizes
+ * return 1. Its first call on a device looks up the array's device address
+ * and may load the module (make it at start-up, before any stream capture);
+ * all calls share the array, so calls that overlap on the GPU race (order
+ * them on one stream). Returns 0 on success, 4 for a launch error of this
+ * call, 5 when an earlier CUDA error is pending (nothing queued). */
 int ipm_deposit_noalloc(const double* verts, long long ncx, long long ncy, IPM_DTYPE factor, int npx, int npy,
                         IPM_DTYPE* map, void* stream);
 

@@ -228,9 +228,12 @@ bool copy_fixed_maps(Obj* self, unsigned long long* total, unsigned long long* m
 // caller provides, and its fixed-point scratch lives in the file-scope device
 // array below instead of being allocated.
 //
-// Limit: maps of at most kNoAllocMaxPixels pixels and kNoAllocMaxRows rows
-// (1024 x 1024). The array (16.8 MB) is part of the module, so every GPU that
-// loads this library holds it until the process exits.
+// Limit: maps of at most kNoAllocMaxPixels = 1024 * 1024 pixels in all and at
+// most kNoAllocMaxRows = 1024 rows (so 2048 x 512 is accepted, 1024 x 1025 is
+// not). The array (16.8 MB) is part of the module, so every GPU that loads
+// this library holds it until the process exits; with CUDA's lazy module
+// loading (the default) the first call on a device may load the module,
+// reserving that memory then.
 namespace {
 constexpr long long kNoAllocMaxPixels = 1024LL * 1024LL;
 constexpr long long kNoAllocMaxRows = 1024;
@@ -274,16 +277,22 @@ extern "C" {
 // units. The work is queued on `stream` (a cudaStream_t; NULL for the default
 // stream) and the call returns without waiting for it.
 //
-// Returns 0 on success, 1 for sizes beyond the limit (more than 1024 x 1024
-// pixels or more than 1024 rows) or invalid arguments, 3 if the scratch
-// address cannot be found, 4 for a launch error. The call allocates nothing.
-// Its first call on a device looks up the device address of the scratch
-// array; make that first call before any stream capture. All calls share the
-// one scratch array (cleared at the start of each call), so calls whose work
-// overlaps on the GPU race: order them on one stream or synchronise between
-// them.
+// Returns 0 on success, 1 for sizes beyond the limit (more than 1024 * 1024
+// pixels in all or more than 1024 rows) or invalid arguments, 3 if the
+// scratch address cannot be found, 4 for an error of this call's launches, 5
+// if a CUDA error from earlier work is already pending on the calling thread
+// (nothing is queued and the error is left for its owner to read). The call
+// allocates nothing. Its first call on a device looks up the device address
+// of the scratch array and may load the module: make that first call at
+// start-up, before any stream capture. All calls share the one scratch array
+// (cleared at the start of each call), so calls whose work overlaps on the
+// GPU race: order them on one stream or synchronise between them.
 int ipm_deposit_noalloc(const double* verts, long long ncx, long long ncy, dtype factor, int npx, int npy,
                         dtype* map, void* stream) {
+  if (cudaPeekAtLastError() != cudaSuccess) {
+    std::fprintf(stderr, "ipm_deposit_noalloc: an earlier CUDA error is pending; nothing queued\n");
+    return 5;
+  }
   if (!verts || !map || ncx < 1 || ncy < 1 || npx < 1 || npy < 1) {
     std::fprintf(stderr, "ipm_deposit_noalloc: invalid arguments\n");
     return 1;

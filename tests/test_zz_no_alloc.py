@@ -62,6 +62,25 @@ def test_no_alloc_deposit_matches_allocating_path(gpu, dbl):
 def test_no_alloc_rejects_sizes_beyond_the_limit(gpu):
     lib = irs_b200.IPM(**IPM_SMALL).lib
     fn = _bind(lib, ctypes.c_float)
-    # 2048 x 600 pixels exceeds the 1024 x 1024 limit: rejected before any GPU work
+    # 2048 x 600 pixels exceeds 1024 * 1024 pixels in all: rejected before any GPU work
     assert fn(ctypes.c_void_p(16), 4, 4, 0.5, 2048, 600, ctypes.c_void_p(16), None) == 1
-    assert fn(ctypes.c_void_p(16), 4, 4, 0.5, 64, 2000, ctypes.c_void_p(16), None) == 1
+    # 1025 rows exceed the 1024-row limit
+    assert fn(ctypes.c_void_p(16), 4, 4, 0.5, 64, 1025, ctypes.c_void_p(16), None) == 1
+
+
+def test_no_alloc_accepts_a_wide_map(gpu):
+    """2048 x 512 pixels: within 1024 * 1024 pixels in all and 1024 rows. A
+    coarse unit lattice over the map deposits one unit of area per pixel."""
+    import torch
+    lib = irs_b200.IPM(**IPM_SMALL).lib
+    fn = _bind(lib, ctypes.c_float)
+    npx, npy = 2048, 512
+    v = np.stack(np.meshgrid(np.arange(0, npx + 1, 4.0), np.arange(0, npy + 1, 4.0)), -1)
+    d_v = torch.from_numpy(np.ascontiguousarray(v)).to("cuda")
+    d_map = torch.full((npy, npx), -1.0, dtype=torch.float32, device="cuda")
+    # each 4 x 4 cell has area 16 = two triangles of 8: factor 8 spreads 1 per pixel
+    rc = fn(d_v.data_ptr(), v.shape[1] - 1, v.shape[0] - 1, 8.0, npx, npy, d_map.data_ptr(),
+            torch.cuda.current_stream().cuda_stream)
+    assert rc == 0
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(d_map.cpu().numpy(), np.ones((npy, npx), np.float32), rtol=0, atol=1e-6)
