@@ -24,9 +24,10 @@
 //     lower-left pixel; the map accumulates unsigned 64-bit fixed point (2^32
 //     per unit) with integer atomics, so the result does not depend on thread
 //     order: given the same corner positions the map is bit-exact.
-// Every floating-point operation is an explicitly rounded intrinsic (no FMA
-// contraction), so a host implementation with the same operation sequence
-// reproduces the map bit for bit.
+// Every floating-point operation is an explicitly rounded intrinsic (fused
+// multiply-adds only where written, no contraction by the compiler), so a host
+// implementation with the same operation sequence reproduces the map bit for
+// bit.
 #pragma once
 #include "common.cuh"
 
@@ -43,6 +44,7 @@ struct RN<float> {
   static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
   static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
   static __device__ __forceinline__ float rcp(float a) { return __frcp_rn(a); }
+  static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
   static __device__ __forceinline__ unsigned long long to_fix(float a) {
     return (unsigned long long)__float2ll_rn(a);
   }
@@ -54,6 +56,7 @@ struct RN<double> {
   static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
   static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
   static __device__ __forceinline__ double rcp(double a) { return __drcp_rn(a); }
+  static __device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
   static __device__ __forceinline__ unsigned long long to_fix(double a) {
     return (unsigned long long)__double2ll_rn(a);
   }
@@ -113,9 +116,9 @@ __device__ __forceinline__ Tri<D> setup_head(double ax, double ay, double bx, do
   D x0 = D(ax - fx), y0 = D(ay - fy), x1 = D(bx - fx), y1 = D(by - fy), x2 = D(cx - fx), y2 = D(cy - fy);
   // shoelace, as Poly::area
   D s = D(0);
-  s = RN<D>::add(s, RN<D>::sub(RN<D>::mul(RN<D>::sub(y1, y0), x0), RN<D>::mul(RN<D>::sub(x1, x0), y0)));
-  s = RN<D>::add(s, RN<D>::sub(RN<D>::mul(RN<D>::sub(y2, y1), x1), RN<D>::mul(RN<D>::sub(x2, x1), y1)));
-  s = RN<D>::add(s, RN<D>::sub(RN<D>::mul(RN<D>::sub(y0, y2), x2), RN<D>::mul(RN<D>::sub(x0, x2), y2)));
+  s = RN<D>::add(s, RN<D>::fma(RN<D>::sub(y1, y0), x0, -RN<D>::mul(RN<D>::sub(x1, x0), y0)));
+  s = RN<D>::add(s, RN<D>::fma(RN<D>::sub(y2, y1), x1, -RN<D>::mul(RN<D>::sub(x2, x1), y1)));
+  s = RN<D>::add(s, RN<D>::fma(RN<D>::sub(y0, y2), x2, -RN<D>::mul(RN<D>::sub(x0, x2), y2)));
   D A = RN<D>::mul(s, D(0.5));  // the correctly rounded s / 2, as a division gives
   if (!(dabs(A) < RN<D>::mul(D(10000), factor))) return t;
   D whole = dabs(A);
@@ -247,11 +250,11 @@ __device__ __forceinline__ bool row_geometry(const Tri<D>& t, D rb, D rt, Strip<
     if (dy != D(0)) {
       const D ta = RN<D>::mul(RN<D>::sub(rb, y1), t.idy[k]), tb = RN<D>::mul(RN<D>::sub(rt, y1), t.idy[k]);
       if (on_b) {
-        const D p = RN<D>::add(x1, RN<D>::mul(ta, dx));
+        const D p = RN<D>::fma(ta, dx, x1);
         extend(hb, cb0, cb1, p, p);
       }
       if (on_t) {
-        const D p = RN<D>::add(x1, RN<D>::mul(tb, dx));
+        const D p = RN<D>::fma(tb, dx, x1);
         extend(ht, ct0, ct1, p, p);
       }
       const D lo = ta < tb ? ta : tb, hi = ta > tb ? ta : tb;
@@ -265,10 +268,10 @@ __device__ __forceinline__ bool row_geometry(const Tri<D>& t, D rb, D rt, Strip<
     }
     D xa = D(0), ya = D(0), xb = D(0), yb = D(0);
     if (ok) {
-      xa = RN<D>::add(x1, RN<D>::mul(t0, dx));
-      xb = RN<D>::add(x1, RN<D>::mul(t1, dx));
-      ya = RN<D>::sub(RN<D>::add(y1, RN<D>::mul(t0, dy)), rb);
-      yb = RN<D>::sub(RN<D>::add(y1, RN<D>::mul(t1, dy)), rb);
+      xa = RN<D>::fma(t0, dx, x1);
+      xb = RN<D>::fma(t1, dx, x1);
+      ya = RN<D>::sub(RN<D>::fma(t0, dy, y1), rb);
+      yb = RN<D>::sub(RN<D>::fma(t1, dy, y1), rb);
       extend(any, xlo, xhi, xa, xb);
     }
     g.xa[k] = xa;
@@ -298,9 +301,9 @@ __device__ __forceinline__ D pixel_coverage(const Tri<D>& t, const Strip<D>& g, 
     xe = xe < c1 ? xe : c1;
     const D w = RN<D>::sub(xe, xs);
     if (w != D(0)) {
-      const D ys = RN<D>::add(g.ya[k], RN<D>::mul(RN<D>::sub(xs, g.xa[k]), t.sl[k]));
-      const D ye = RN<D>::add(g.ya[k], RN<D>::mul(RN<D>::sub(xe, g.xa[k]), t.sl[k]));
-      s = RN<D>::sub(s, RN<D>::mul(RN<D>::mul(w, RN<D>::add(ys, ye)), D(0.5)));
+      const D ys = RN<D>::fma(RN<D>::sub(xs, g.xa[k]), t.sl[k], g.ya[k]);
+      const D ye = RN<D>::fma(RN<D>::sub(xe, g.xa[k]), t.sl[k], g.ya[k]);
+      s = RN<D>::fma(RN<D>::mul(w, D(-0.5)), RN<D>::add(ys, ye), s);
     }
   }
   if (has_top) {

@@ -980,21 +980,25 @@ void orc_ipm_deposit_ref(long long ncx, long long ncy, const double* vx, const d
 #define D float
 #define SUF f32
 #define RINT llrintf
+#define FMA fmaf
 #define DMAX FLT_MAX
 #include "fixdep.inc"
 #undef D
 #undef SUF
 #undef RINT
+#undef FMA
 #undef DMAX
 
 #define D double
 #define SUF f64
 #define RINT llrint
+#define FMA fma
 #define DMAX DBL_MAX
 #include "fixdep.inc"
 #undef D
 #undef SUF
 #undef RINT
+#undef FMA
 #undef DMAX
 
 /* ------------------------------------------------------------ derived parameters (double) */
