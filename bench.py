@@ -442,10 +442,10 @@ def reference_arm(args):
 
 def batch_measure(steps):
     """The batched form: 256 realizations of uneven size (1024^2 maps, half
-    length 12) through the graph-captured pipeline, timed per replay; then the
+    length 12) through the graph-captured pipeline, its best replay; then the
     plain uniform FP64 form of every realization run singly at the same
-    expansion order, timed by its device pipeline, and the FP32 batch maps'
-    error against those FP64 maps."""
+    expansion order, the best of two runs of its device pipeline each, and the
+    FP32 batch maps' error against those FP64 maps."""
     import irs_b200
     from irs_b200.batch import random_realizations
 
@@ -455,7 +455,7 @@ def batch_measure(steps):
     b.run()
     first = time.perf_counter() - t0
     ts = [b.rerun(1) for _ in range(max(2, steps))]
-    t_batch = float(np.mean(ts))
+    t_batch = float(np.min(ts))
     pix, cells = b.value("total_pixels"), b.value("total_cells")
     order = int(b.value("expansion_order"))
     maps = b.maps
@@ -469,7 +469,7 @@ def batch_measure(steps):
     for r, kw in enumerate(reals):
         s = irs_b200.IPM(**kw, is_double=True, expansion_order=order)
         s.run()
-        t_plain += s.rerun(1)
+        t_plain += min(s.rerun(1), s.rerun(1))  # best of two, as the batch's best replay
         ref = s.magnifications
         s.close()
         ok = ref > 0
