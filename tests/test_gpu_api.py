@@ -31,6 +31,25 @@ def test_ipm_run_and_save_files(gpu, tmp_path):
     assert int(info["num_stars"]) == m.num_stars
 
 
+def test_saved_files_read_back_through_util(gpu, tmp_path):
+    """The files save() writes, read with irs_b200.util (the reference's
+    helper-module interface), give back the run's map, stars and parameters."""
+    from irs_b200 import util
+    m = irs_b200.IPM(**{**IPM_SMALL, "write_histograms": 1}, outfile_prefix=str(tmp_path) + "/")
+    m.run()
+    m.save()
+    np.testing.assert_array_equal(util.read_array(str(tmp_path / "ipm_magnifications.bin"), np.float32),
+                                  m.magnifications)
+    stars, rect, corner, theta = util.read_stars(str(tmp_path / "ipm_stars.bin"))
+    np.testing.assert_array_equal(stars, m.stars)
+    assert rect == bool(IPM_SMALL.get("rectangular", False))
+    assert theta == np.float32(m.theta_star)
+    info = util.read_params(str(tmp_path / "ipm_parameter_info.txt"))
+    assert info["num_stars"] == m.num_stars and isinstance(info["num_stars"], int)
+    hist = util.read_hist(str(tmp_path / "ipm_mags_numpixels.txt"))
+    assert hist.dtype == np.int32 and hist[:, 1].sum() == m.magnifications.size
+
+
 def test_star_generation_statistics(gpu):
     m = irs_b200.IPM(**IPM_SMALL, is_double=True)
     m.run()
