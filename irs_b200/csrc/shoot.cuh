@@ -24,7 +24,9 @@
 // and <= 31 coefficients in shared memory, and every lane reads them as
 // warp-wide broadcasts. Each thread evaluates 4 lattice points (rows ty,
 // ty+8, ty+16, ty+24 of the tile) against each staged star, so one
-// shared-memory read feeds 4 evaluations.
+// shared-memory read feeds 4 evaluations. Without parities the FP32 form runs
+// its near and far field on pairs of points with the paired FP32 instructions
+// of sm_100 (near_far_pairs): half the issue slots, the same bits.
 //
 // Outputs: IRS adds one count per ray to the int32 map with the reference's
 // clamp and row flip (irs_functions.cuh:147-198); the IPM vertex mode writes
@@ -140,6 +142,50 @@ __device__ __forceinline__ float rcp_approx(float x) {
   return r;
 }
 
+// Two FP32 values in one 64-bit register pair. The paired (.f32x2) add, sub,
+// mul and fma of sm_100 round each half exactly as the scalar instruction
+// does, with one issue slot for both: the FP32 lens kernel evaluates two
+// lattice points per instruction with results bit-identical to the scalar form.
+struct f32x2 {
+  unsigned long long v;
+};
+__device__ __forceinline__ f32x2 pk2(float lo, float hi) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void upk2(f32x2 a, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a.v));
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+  return r;
+}
+
+// A leaf's near stars and expansion coefficients staged for the paired form:
+// each value twice, so that one shared-memory load gives both halves.
+struct NearPairs {
+  ulonglong2 xy[kMaxStarsDirect];  // (x, x), (y, y)
+  unsigned long long m[kMaxStarsDirect];  // (m, m)
+  ulonglong2 coef[kMaxOrder];  // (re, re), (im, im)
+};
+
 // Adds one ray count with the reference's clamp and row flip; (px, py) are the
 // source position in pixel units (unflipped).
 __device__ __forceinline__ void irs_deposit(double px, double py, int npx, int npy, int* __restrict__ pix,
@@ -253,12 +299,101 @@ __global__ void __launch_bounds__(kShootThreads) shoot_f64(ShootParams sp, LeafP
 }
 
 // ----------------------------------------------------------------- FP32 form
+// Near-field sums and far-field Horner values of R lattice points sharing the
+// column offset ux (rows uy[0..R-1], R even), on pairs of points: the same
+// operations in the same order as the scalar form of shoot_f32_tile, so the
+// results are the same bits. fmaf(-Ai, dzi, c) is written fma(Ai, -dzi, c),
+// the same product.
+template <int R>
+__device__ __forceinline__ void near_far_pairs(float ux, const float* uy, float inv_hl, int nn4, int p,
+                                               const NearPairs& sp2, float* sx, float* sy, float* cxr, float* cyr,
+                                               float* Ar, float* Ai) {
+  constexpr int P = R / 2;
+  const f32x2 zero = pk2(0.f, 0.f), ux2 = pk2(ux, ux);
+  f32x2 uy2[P], Sx[P], Sy[P], Cx[P], Cy[P];
+#pragma unroll
+  for (int q = 0; q < P; q++) {
+    uy2[q] = pk2(uy[2 * q], uy[2 * q + 1]);
+    Sx[q] = Sy[q] = Cx[q] = Cy[q] = zero;
+  }
+  auto star = [&](int s, f32x2* bx, f32x2* by) {
+    const ulonglong2 xy = sp2.xy[s];
+    const f32x2 xx{xy.x}, yy{xy.y}, mm{sp2.m[s]};
+    const f32x2 ex = sub2(ux2, xx), ex2 = mul2(ex, ex);
+#pragma unroll
+    for (int q = 0; q < P; q++) {
+      const f32x2 ey = sub2(uy2[q], yy);
+      const f32x2 r2 = fma2(ey, ey, ex2);
+      float r2a, r2b;
+      upk2(r2, r2a, r2b);
+      const f32x2 w = mul2(mm, pk2(rcp_approx(r2a), rcp_approx(r2b)));
+      bx[q] = fma2(w, ex, bx[q]);
+      by[q] = fma2(w, ey, by[q]);
+    }
+  };
+  for (int s0 = 0; s0 < nn4; s0 += 16) {
+    f32x2 bx[P], by[P];
+#pragma unroll
+    for (int q = 0; q < P; q++) bx[q] = by[q] = zero;
+#pragma unroll
+    for (int s = 0; s < 4; s++) star(s0 + s, bx, by);
+#pragma unroll
+    for (int g = 1; g < 4; g++) {
+      if (s0 + 4 * (g + 1) <= nn4) {
+#pragma unroll
+        for (int s = 0; s < 4; s++) star(s0 + 4 * g + s, bx, by);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < P; q++) {  // two-sum of the block into the running sum
+      f32x2 t = add2(Sx[q], bx[q]);
+      f32x2 bb = sub2(t, Sx[q]);
+      Cx[q] = add2(Cx[q], add2(sub2(Sx[q], sub2(t, bb)), sub2(bx[q], bb)));
+      Sx[q] = t;
+      t = add2(Sy[q], by[q]);
+      bb = sub2(t, Sy[q]);
+      Cy[q] = add2(Cy[q], add2(sub2(Sy[q], sub2(t, bb)), sub2(by[q], bb)));
+      Sy[q] = t;
+    }
+  }
+  const float dzr = ux * inv_hl;
+  const f32x2 dzr2 = pk2(dzr, dzr);
+  f32x2 dzi2[P], ndzi2[P], A[P], B[P];
+#pragma unroll
+  for (int q = 0; q < P; q++) {
+    const float a = uy[2 * q] * inv_hl, b = uy[2 * q + 1] * inv_hl;
+    dzi2[q] = pk2(a, b);
+    ndzi2[q] = pk2(-a, -b);
+    A[q] = B[q] = zero;
+  }
+  for (int k = p - 1; k >= 0; k--) {
+    const ulonglong2 c = sp2.coef[k];
+    const f32x2 cr{c.x}, ci{c.y};
+#pragma unroll
+    for (int q = 0; q < P; q++) {
+      const f32x2 ar = fma2(A[q], dzr2, fma2(B[q], ndzi2[q], cr));
+      B[q] = fma2(A[q], dzi2[q], fma2(B[q], dzr2, ci));
+      A[q] = ar;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < P; q++) {
+    upk2(Sx[q], sx[2 * q], sx[2 * q + 1]);
+    upk2(Sy[q], sy[2 * q], sy[2 * q + 1]);
+    upk2(Cx[q], cxr[2 * q], cxr[2 * q + 1]);
+    upk2(Cy[q], cyr[2 * q], cyr[2 * q + 1]);
+    upk2(A[q], Ar[2 * q], Ar[2 * q + 1]);
+    upk2(B[q], Ai[2 * q], Ai[2 * q + 1]);
+  }
+}
+
 // GENERIC_SMOOTH: the smooth sheet is not the circular approximation
 // (alpha_smooth = -kappa_star z); its deviation from that linear form is then
 // added per point in FP64.
 template <bool VERT, bool PAR, bool GENERIC_SMOOTH, int THREADS = kShootThreads>
 __device__ __forceinline__ void shoot_f32_tile(const ShootParams& sp, const LeafPtrs& lp, const TileInfo& ti,
-                                               const ShootOut& o, float4* s_near, float2* s_coef) {
+                                               const ShootOut& o, float4* s_near, float2* s_coef,
+                                               NearPairs* s_pair) {
   static_assert(THREADS >= 128 && THREADS <= 1024 && kTileY % (THREADS / kTileX) == 0, "tile shape");
   constexpr int R = kTileY / (THREADS / kTileX);  // lattice points per thread
   constexpr int RS = THREADS / kTileX;            // row stride between a thread's points
@@ -275,9 +410,14 @@ __device__ __forceinline__ void shoot_f32_tile(const ShootParams& sp, const Leaf
       float4 v = lp.near32[(size_t)ti.leaf * kMaxStarsDirect + threadIdx.x];
       if (threadIdx.x >= nn) v = make_float4(1e18f, 1e18f, 0.f, 0.f);  // far away, zero mass
       s_near[threadIdx.x] = v;
+      s_pair->xy[threadIdx.x] = make_ulonglong2(pk2(v.x, v.x).v, pk2(v.y, v.y).v);
+      s_pair->m[threadIdx.x] = pk2(v.z, v.z).v;
     }
-    if (threadIdx.x >= 64 && threadIdx.x < 64 + kMaxOrder)
-      s_coef[threadIdx.x - 64] = lp.coef32[(size_t)ti.leaf * kMaxOrder + threadIdx.x - 64];
+    if (threadIdx.x >= 64 && threadIdx.x < 64 + kMaxOrder) {
+      const float2 c = lp.coef32[(size_t)ti.leaf * kMaxOrder + threadIdx.x - 64];
+      s_coef[threadIdx.x - 64] = c;
+      s_pair->coef[threadIdx.x - 64] = make_ulonglong2(pk2(c.x, c.x).v, pk2(c.y, c.y).v);
+    }
     const double lcx = lp.cx[ti.leaf], lcy = lp.cy[ti.leaf];
     const float inv_hl = float(1.0 / lp.hl[ti.leaf]);
     // leaf-centre part of the source position, in pixel units
@@ -299,79 +439,85 @@ __device__ __forceinline__ void shoot_f32_tile(const ShootParams& sp, const Leaf
 #pragma unroll
       for (int r = 0; r < R; r++)  // each row from its own index: independent of the tiling
         uy[r] = float((sp.base_y + 2.0 * (sp.rhs_y * double(j0 + r * RS))) - lcy);
-      // ---- near field, blocked compensated summation
       float sx[R], sy[R], cxr[R], cyr[R];
       float dxx[R], dxy[R];  // derivative sums (parity only)
+      float Ar[R], Ai[R], Dr[R], Di[R];
+      if constexpr (!PAR && R % 2 == 0) {
+        // the same operations on pairs of points (rows r, r + 1)
+        near_far_pairs<R>(ux, uy, inv_hl, nn4, sp.p, *s_pair, sx, sy, cxr, cyr, Ar, Ai);
+      } else {
+        // ---- near field, blocked compensated summation
 #pragma unroll
-      for (int r = 0; r < R; r++) sx[r] = sy[r] = cxr[r] = cyr[r] = dxx[r] = dxy[r] = 0.f;
-      // blocks of 16 stars (the last one of 4, 8 or 12 when nn4 is not a
-      // multiple of 16), each block's sum added to the running sum by a
-      // two-sum; a thread's points share ux, so ex and ex^2 are formed once
-      // per star
-      auto star = [&](const float4 st, float* bx, float* by) {
-        const float ex = ux - st.x, ex2 = ex * ex;
+        for (int r = 0; r < R; r++) sx[r] = sy[r] = cxr[r] = cyr[r] = dxx[r] = dxy[r] = 0.f;
+        // blocks of 16 stars (the last one of 4, 8 or 12 when nn4 is not a
+        // multiple of 16), each block's sum added to the running sum by a
+        // two-sum; a thread's points share ux, so ex and ex^2 are formed once
+        // per star
+        auto star = [&](const float4 st, float* bx, float* by) {
+          const float ex = ux - st.x, ex2 = ex * ex;
+#pragma unroll
+          for (int r = 0; r < R; r++) {
+            float ey = uy[r] - st.y;
+            float r2 = fmaf(ey, ey, ex2);
+            float inv = rcp_approx(r2);
+            float q = st.z * inv;
+            bx[r] = fmaf(q, ex, bx[r]);
+            by[r] = fmaf(q, ey, by[r]);
+            if (PAR) {
+              float t2 = q * inv;
+              dxx[r] = fmaf(t2, (ex - ey) * (ex + ey), dxx[r]);
+              dxy[r] = fmaf(t2, 2.f * ex * ey, dxy[r]);
+            }
+          }
+        };
+        for (int s0 = 0; s0 < nn4; s0 += 16) {
+          float bx[R], by[R];
+#pragma unroll
+          for (int r = 0; r < R; r++) bx[r] = by[r] = 0.f;
+#pragma unroll
+          for (int s = 0; s < 4; s++) star(s_near[s0 + s], bx, by);
+#pragma unroll
+          for (int g = 1; g < 4; g++) {
+            if (s0 + 4 * (g + 1) <= nn4) {
+#pragma unroll
+              for (int s = 0; s < 4; s++) star(s_near[s0 + 4 * g + s], bx, by);
+            }
+          }
+#pragma unroll
+          for (int r = 0; r < R; r++) {  // two-sum of the block into the running sum
+            float s = sx[r] + bx[r];
+            float bb = s - sx[r];
+            cxr[r] += (sx[r] - (s - bb)) + (bx[r] - bb);
+            sx[r] = s;
+            s = sy[r] + by[r];
+            bb = s - sy[r];
+            cyr[r] += (sy[r] - (s - bb)) + (by[r] - bb);
+            sy[r] = s;
+          }
+        }
+        // ---- far field: Horner in dz = u / hl, one coefficient read per 4 points
+        float dzr[R], dzi[R];
 #pragma unroll
         for (int r = 0; r < R; r++) {
-          float ey = uy[r] - st.y;
-          float r2 = fmaf(ey, ey, ex2);
-          float inv = rcp_approx(r2);
-          float q = st.z * inv;
-          bx[r] = fmaf(q, ex, bx[r]);
-          by[r] = fmaf(q, ey, by[r]);
-          if (PAR) {
-            float t2 = q * inv;
-            dxx[r] = fmaf(t2, (ex - ey) * (ex + ey), dxx[r]);
-            dxy[r] = fmaf(t2, 2.f * ex * ey, dxy[r]);
-          }
+          dzr[r] = ux * inv_hl;
+          dzi[r] = uy[r] * inv_hl;
+          Ar[r] = Ai[r] = Dr[r] = Di[r] = 0.f;
         }
-      };
-      for (int s0 = 0; s0 < nn4; s0 += 16) {
-        float bx[R], by[R];
+        for (int k = sp.p - 1; k >= 0; k--) {
+          const float2 c = s_coef[k];
 #pragma unroll
-        for (int r = 0; r < R; r++) bx[r] = by[r] = 0.f;
-#pragma unroll
-        for (int s = 0; s < 4; s++) star(s_near[s0 + s], bx, by);
-#pragma unroll
-        for (int g = 1; g < 4; g++) {
-          if (s0 + 4 * (g + 1) <= nn4) {
-#pragma unroll
-            for (int s = 0; s < 4; s++) star(s_near[s0 + 4 * g + s], bx, by);
+          for (int r = 0; r < R; r++) {
+            if (PAR && k >= 1) {  // derivative polynomial sum k e_k dz^(k-1)
+              float tr = fmaf(Dr[r], dzr[r], -Di[r] * dzi[r]);
+              float tt = fmaf(Dr[r], dzi[r], Di[r] * dzr[r]);
+              Dr[r] = fmaf(c.x, float(k), tr);
+              Di[r] = fmaf(c.y, float(k), tt);
+            }
+            // A <- A dz + c as two FMA chains (4 operations per order)
+            const float ar = fmaf(Ar[r], dzr[r], fmaf(-Ai[r], dzi[r], c.x));
+            Ai[r] = fmaf(Ar[r], dzi[r], fmaf(Ai[r], dzr[r], c.y));
+            Ar[r] = ar;
           }
-        }
-#pragma unroll
-        for (int r = 0; r < R; r++) {  // two-sum of the block into the running sum
-          float s = sx[r] + bx[r];
-          float bb = s - sx[r];
-          cxr[r] += (sx[r] - (s - bb)) + (bx[r] - bb);
-          sx[r] = s;
-          s = sy[r] + by[r];
-          bb = s - sy[r];
-          cyr[r] += (sy[r] - (s - bb)) + (by[r] - bb);
-          sy[r] = s;
-        }
-      }
-      // ---- far field: Horner in dz = u / hl, one coefficient read per 4 points
-      float Ar[R], Ai[R], Dr[R], Di[R], dzr[R], dzi[R];
-#pragma unroll
-      for (int r = 0; r < R; r++) {
-        dzr[r] = ux * inv_hl;
-        dzi[r] = uy[r] * inv_hl;
-        Ar[r] = Ai[r] = Dr[r] = Di[r] = 0.f;
-      }
-      for (int k = sp.p - 1; k >= 0; k--) {
-        const float2 c = s_coef[k];
-#pragma unroll
-        for (int r = 0; r < R; r++) {
-          if (PAR && k >= 1) {  // derivative polynomial sum k e_k dz^(k-1)
-            float tr = fmaf(Dr[r], dzr[r], -Di[r] * dzi[r]);
-            float tt = fmaf(Dr[r], dzi[r], Di[r] * dzr[r]);
-            Dr[r] = fmaf(c.x, float(k), tr);
-            Di[r] = fmaf(c.y, float(k), tt);
-          }
-          // A <- A dz + c as two FMA chains (4 operations per order)
-          const float ar = fmaf(Ar[r], dzr[r], fmaf(-Ai[r], dzi[r], c.x));
-          Ai[r] = fmaf(Ar[r], dzi[r], fmaf(Ai[r], dzr[r], c.y));
-          Ar[r] = ar;
         }
       }
       // ---- output
@@ -432,9 +578,10 @@ __global__ void __launch_bounds__(THREADS) shoot_f32(ShootParams sp, LeafPtrs lp
                                                      int* __restrict__ psad, double2* __restrict__ verts) {
   __shared__ float4 s_near[kMaxStarsDirect];
   __shared__ float2 s_coef[kMaxOrder];
+  __shared__ NearPairs s_pair;
   const ShootOut o{pix, pmin, psad, verts, sp.jbase};
   for (long long t = blockIdx.x; t < total_tiles; t += gridDim.x)
-    shoot_f32_tile<VERT, PAR, GENERIC_SMOOTH, THREADS>(sp, lp, tile_info(lp, t), o, s_near, s_coef);
+    shoot_f32_tile<VERT, PAR, GENERIC_SMOOTH, THREADS>(sp, lp, tile_info(lp, t), o, s_near, s_coef, &s_pair);
 }
 
 // The level-s corner lattice restricted to refined tiles: work items whose
@@ -444,6 +591,7 @@ __global__ void __launch_bounds__(kShootThreads) shoot_f32_tiles(ShootParams sp,
                                                                  TileStore st) {
   __shared__ float4 s_near[kMaxStarsDirect];
   __shared__ float2 s_coef[kMaxOrder];
+  __shared__ NearPairs s_pair;
   const ShootOut o{nullptr, nullptr, nullptr, nullptr, 0, &st};
   const long long side = 32LL * st.s;
   for (long long t = blockIdx.x; t < total_tiles; t += gridDim.x) {
@@ -455,7 +603,7 @@ __global__ void __launch_bounds__(kShootThreads) shoot_f32_tiles(ShootParams sp,
       for (int tx = tx0 > 0 ? tx0 - 1 : 0; tx <= tx1 && tx < st.ntx && !need; tx++)
         need = st.slot[ty * st.ntx + tx] >= 0;
     if (!need) continue;
-    shoot_f32_tile<true, false, GENERIC_SMOOTH>(sp, lp, ti, o, s_near, s_coef);
+    shoot_f32_tile<true, false, GENERIC_SMOOTH>(sp, lp, ti, o, s_near, s_coef, &s_pair);
   }
 }
 
@@ -477,13 +625,14 @@ __global__ void __launch_bounds__(kShootThreads) shoot_f32_batch(BatchShoot bs, 
                                                                  double2* __restrict__ verts) {
   __shared__ float4 s_near[kMaxStarsDirect];
   __shared__ float2 s_coef[kMaxOrder];
+  __shared__ NearPairs s_pair;
   if (*bs.err & kErrTableOverflow) return;
   const long long total = *bs.total < bs.table_cap ? *bs.total : bs.table_cap;
   for (long long t = blockIdx.x; t < total; t += gridDim.x) {
     const TileInfo ti = tile_info(lp, t);
     const int r = bs.leaf_rid[ti.leaf];
     const ShootOut o{nullptr, nullptr, nullptr, verts + bs.voff[r], bs.vrow0[r]};
-    shoot_f32_tile<true, false, GENERIC_SMOOTH>(bs.sps[r], lp, ti, o, s_near, s_coef);
+    shoot_f32_tile<true, false, GENERIC_SMOOTH>(bs.sps[r], lp, ti, o, s_near, s_coef, &s_pair);
   }
 }
 
