@@ -110,7 +110,7 @@ void set_stars(IPMHandle* self, const IPM_DTYPE* xym, int n, int rectangular, IP
 double get_t_pipeline(IPMHandle* self);               /* seconds: tree + expansions + shoot */
 bool rerun(IPMHandle* self, int repeats, double* seconds); /* re-run tree+expansions+shoot on the resident stars */
 void set_band(IPMHandle* self, long long first, long long last); /* lattice row band [first, last); last < 0: all */
-void set_shoot_launch(IPMHandle* self, int threads, int ctas_per_sm); /* FP32 lens-equation kernel: 128/256/512 threads per CTA (8/4/2 lattice points per thread), CTAs per SM */
+void set_shoot_launch(IPMHandle* self, int threads, int ctas_per_sm); /* FP32 lens-equation kernel: 128/256/512 threads per CTA (8/4/2 lattice points per thread), CTAs per SM of its grid; other values: 128 and 64 */
 int get_shoot_threads(IPMHandle* self);
 int get_shoot_ctas_per_sm(IPMHandle* self);
 bool copy_maps_device(IPMHandle* self, void* total, void* minima, void* saddles); /* integer maps to device buffers */

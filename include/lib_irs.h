@@ -102,7 +102,7 @@ void set_stars(IRSHandle* self, const IRS_DTYPE* xym, int n, int rectangular, IR
 double get_t_pipeline(IRSHandle* self);
 bool rerun(IRSHandle* self, int repeats, double* seconds); /* re-run tree+expansions+shoot on the resident stars */
 void set_band(IRSHandle* self, long long first, long long last); /* lattice row band [first, last); last < 0: all */
-void set_shoot_launch(IRSHandle* self, int threads, int ctas_per_sm); /* FP32 lens-equation kernel: 128/256/512 threads per CTA (8/4/2 lattice points per thread), CTAs per SM */
+void set_shoot_launch(IRSHandle* self, int threads, int ctas_per_sm); /* FP32 lens-equation kernel: 128/256/512 threads per CTA (8/4/2 lattice points per thread), CTAs per SM of its grid; other values: 128 and 64 */
 int get_shoot_threads(IRSHandle* self);
 int get_shoot_ctas_per_sm(IRSHandle* self);
 bool copy_maps_device(IRSHandle* self, void* total, void* minima, void* saddles); /* integer maps to device buffers */

@@ -23,7 +23,7 @@ import numpy as np
 from .mapmaker import IPM
 
 THREADS = (128, 256, 512)
-CTAS_PER_SM = (4, 8, 16)
+CTAS_PER_SM = (8, 16, 32, 64)
 
 
 def autotune(config: dict, band_rows: int = 256, target_px: float | None = None, orders=None, threads=THREADS,

@@ -102,8 +102,9 @@ int get_expansion_order(Obj* self) { return self->prm.expansion_order; }
 // 0: default form (FP32 for float libraries, FP64 for double ones), 1: FP64, 2: FP32
 void set_precision(Obj* self, int mode) { self->precision = mode; }
 void set_shoot_launch(Obj* self, int threads, int ctas_per_sm) {
-  self->shoot_threads = (threads == 128 || threads == 512) ? threads : 256;
-  self->shoot_ctas_per_sm = ctas_per_sm > 0 ? ctas_per_sm : 8;
+  // anything else than 128, 256 or 512 threads, or CTAs per SM <= 0: the default
+  self->shoot_threads = (threads == 128 || threads == 256 || threads == 512) ? threads : 128;
+  self->shoot_ctas_per_sm = ctas_per_sm > 0 ? ctas_per_sm : 64;
 }
 int get_shoot_threads(Obj* self) { return self->shoot_threads; }
 int get_shoot_ctas_per_sm(Obj* self) { return self->shoot_ctas_per_sm; }
