@@ -324,8 +324,8 @@ class AdaptiveIPM {
       if (!pieces.empty()) {
         IRSB_CKR(cudaMemcpyAsync(d_pieces_.p, pieces.data(), pieces.size() * sizeof(DepositPiece<float>),
                                  cudaMemcpyHostToDevice, s));
-        const int gd = int(std::max<long long>(1, std::min<long long>(ceil_div(nchunks, 8), 148LL * 32)));
-        ipm_deposit_batch<float><<<gd, 256, 0, s>>>(d_ref_.p, d_pieces_.p, int(pieces.size()), nchunks, ws, ws, M,
+        const int gd = deposit_grid(nchunks);
+        ipm_deposit_batch<float><<<gd, kDepositThreads, 0, s>>>(d_ref_.p, d_pieces_.p, int(pieces.size()), nchunks, ws, ws, M,
                                                     W2, WD);
         const int gr = std::max(1, std::min(ceil_div((long long)ws * 5 * n * 32, 256), 148 * 8));
         ipm_resolve_rows<<<gr, 256, 0, s>>>(ws, ws * 5 * n, M);
@@ -351,8 +351,8 @@ class AdaptiveIPM {
     IRSB_CKR(cudaMemsetAsync(d_bdiff_.p, 0, ndiff * sizeof(unsigned long long), s));
     const DepositMaps M{d_bacc_.p, d_bdiff_.p};
     const long long ncells = g_.ncx * g_.ncy;
-    const int grid = int(std::max<long long>(1, std::min<long long>((ncells + 255) / 256, 148LL * 16)));
-    ipm_deposit_cells<float><<<grid, 256, 0, s>>>(base.d_verts_.p, g_.ncx, g_.ncy, ipm_triangle_factor<T, float>(p),
+    const int grid = deposit_grid((ncells + 31) / 32);
+    ipm_deposit_cells<float><<<grid, kDepositThreads, 0, s>>>(base.d_verts_.p, g_.ncx, g_.ncy, ipm_triangle_factor<T, float>(p),
                                                   npx, npy, M, M, M, 0);
     const int gr = std::max(1, std::min(ceil_div((long long)npy * 32, 256), 148 * 8));
     ipm_resolve_rows<<<gr, 256, 0, s>>>(npx, npy, M);
@@ -554,8 +554,8 @@ class AdaptiveIPM {
         IRSB_LAUNCH_CK("ada_refine_tiles");
         verts = d_ref_.p;
       }
-      const int grid = int(std::max<long long>(1, std::min<long long>(ceil_div(L.nchunks, 8), 148LL * 32)));
-      ipm_deposit_batch<float><<<grid, 256, 0, s>>>(verts, d_pieces_.p + L.piece_off, int(L.npieces), L.nchunks, npx,
+      const int grid = deposit_grid(L.nchunks);
+      ipm_deposit_batch<float><<<grid, kDepositThreads, 0, s>>>(verts, d_pieces_.p + L.piece_off, int(L.npieces), L.nchunks, npx,
                                                     npy, M, 0, 0);
       IRSB_LAUNCH_CK("ada deposit");
     }

@@ -632,8 +632,8 @@ class BatchMaker {
       else
         shoot_f32_batch<false><<<148 * 8, kShootThreads, 0, s>>>(bs, lp, d_verts_.p);
       const PassPlan& pp = pass_[c];
-      const int grid = int(std::max<long long>(1, std::min<long long>(ceil_div(pp.nchunks, 8), 148LL * 32)));
-      ipm_deposit_batch<float><<<grid, 256, 0, s>>>(d_verts_.p, d_pieces_.p + pp.poff, pp.npieces, pp.nchunks, npx_,
+      const int grid = deposit_grid(pp.nchunks);
+      ipm_deposit_batch<float><<<grid, kDepositThreads, 0, s>>>(d_verts_.p, d_pieces_.p + pp.poff, pp.npieces, pp.nchunks, npx_,
                                                     npy_, DepositMaps{d_acc_.p, d_diff_.p}, npix, ndiff);
       IRSB_LAUNCH_CK("batch pass");
     }

@@ -313,8 +313,8 @@ int ipm_deposit_noalloc(const double* verts, long long ncx, long long ncy, dtype
   if (cudaMemsetAsync(m.acc, 0, npix * sizeof(unsigned long long), s) != cudaSuccess) return 4;
   if (cudaMemsetAsync(m.diff, 0, ndiff * sizeof(unsigned long long), s) != cudaSuccess) return 4;
   const long long ncells = ncx * ncy;
-  int grid = int(std::max<long long>(1, std::min<long long>((ncells + 255) / 256, 148LL * 16)));
-  irsb::ipm_deposit_cells<dtype><<<grid, 256, 0, s>>>(reinterpret_cast<const double2*>(verts), ncx, ncy, factor,
+  const int grid = irsb::deposit_grid((ncells + 31) / 32);
+  irsb::ipm_deposit_cells<dtype><<<grid, irsb::kDepositThreads, 0, s>>>(reinterpret_cast<const double2*>(verts), ncx, ncy, factor,
                                                       npx, npy, m, m, m, 0);
   int gr = std::max(1, std::min(irsb::ceil_div((long long)npy * 32, 256), 148 * 8));
   irsb::ipm_resolve_rows<<<gr, 256, 0, s>>>(npx, npy, m);

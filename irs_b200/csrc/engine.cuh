@@ -673,14 +673,14 @@ class MapMaker {
       }
       const long long ncx = p.num_ray_threads.re, ncy = band.second - band.first;
       long long ncells = ncx * ncy;
-      int grid = int(std::max<long long>(1, std::min<long long>((ncells + 255) / 256, 148LL * 16)));
+      const int grid = deposit_grid((ncells + 31) / 32);
       if (use_fp32()) {
         const float factor = ipm_triangle_factor<T, float>(p);
-        ipm_deposit_cells<float><<<grid, 256, 0, stream_>>>(d_verts_.p, ncx, ncy, factor, p.num_pixels_y.re,
+        ipm_deposit_cells<float><<<grid, kDepositThreads, 0, stream_>>>(d_verts_.p, ncx, ncy, factor, p.num_pixels_y.re,
                                                             p.num_pixels_y.im, mt, mmin, msad, par ? 1 : 0);
       } else {
         const double factor = ipm_triangle_factor<T, double>(p);
-        ipm_deposit_cells<double><<<grid, 256, 0, stream_>>>(d_verts_.p, ncx, ncy, factor, p.num_pixels_y.re,
+        ipm_deposit_cells<double><<<grid, kDepositThreads, 0, stream_>>>(d_verts_.p, ncx, ncy, factor, p.num_pixels_y.re,
                                                              p.num_pixels_y.im, mt, mmin, msad, par ? 1 : 0);
       }
       IRSB_LAUNCH_CK("ipm_deposit_cells");
