@@ -628,9 +628,9 @@ class BatchMaker {
       BatchShoot bs{d_sps_.p, d_leaf_rid_.p, d_jlo_.p + (long long)c * R, d_voff_.p + (long long)c * R,
                     W.scan.sum.p, table_cap_, dstat + 1};
       if (generic_)
-        shoot_f32_batch<true><<<148 * 8, kShootThreads, 0, s>>>(bs, lp, d_verts_.p);
+        shoot_f32_batch<true><<<148 * 64, kShootBatchThreads, 0, s>>>(bs, lp, d_verts_.p);
       else
-        shoot_f32_batch<false><<<148 * 8, kShootThreads, 0, s>>>(bs, lp, d_verts_.p);
+        shoot_f32_batch<false><<<148 * 64, kShootBatchThreads, 0, s>>>(bs, lp, d_verts_.p);
       const PassPlan& pp = pass_[c];
       const int grid = deposit_grid(pp.nchunks);
       ipm_deposit_batch<float><<<grid, kDepositThreads, 0, s>>>(d_verts_.p, d_pieces_.p + pp.poff, pp.npieces, pp.nchunks, npx_,

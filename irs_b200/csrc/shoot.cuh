@@ -620,8 +620,12 @@ struct BatchShoot {
   const int* err;            // error bits; a table overflow leaves the table unusable
 };
 
+// threads per CTA of the batched lens pass: 8 lattice points per thread, the
+// fastest single-map shape (with a grid of 64 CTAs per SM)
+constexpr int kShootBatchThreads = 128;
+
 template <bool GENERIC_SMOOTH>
-__global__ void __launch_bounds__(kShootThreads) shoot_f32_batch(BatchShoot bs, LeafPtrs lp,
+__global__ void __launch_bounds__(kShootBatchThreads) shoot_f32_batch(BatchShoot bs, LeafPtrs lp,
                                                                  double2* __restrict__ verts) {
   __shared__ float4 s_near[kMaxStarsDirect];
   __shared__ float2 s_coef[kMaxOrder];
@@ -632,7 +636,7 @@ __global__ void __launch_bounds__(kShootThreads) shoot_f32_batch(BatchShoot bs, 
     const TileInfo ti = tile_info(lp, t);
     const int r = bs.leaf_rid[ti.leaf];
     const ShootOut o{nullptr, nullptr, nullptr, verts + bs.voff[r], bs.vrow0[r]};
-    shoot_f32_tile<true, false, GENERIC_SMOOTH>(bs.sps[r], lp, ti, o, s_near, s_coef, &s_pair);
+    shoot_f32_tile<true, false, GENERIC_SMOOTH, kShootBatchThreads>(bs.sps[r], lp, ti, o, s_near, s_coef, &s_pair);
   }
 }
 
