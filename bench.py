@@ -944,7 +944,7 @@ def main():
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
     ap.add_argument("--size", default="full", choices=["full", "small"],
                     help="small: 500 x 500 map at the same pixel scale (for profiler captures)")
-    ap.add_argument("--case", default=None, choices=["config3-irs-band", "adaptive"],
+    ap.add_argument("--case", default=None, choices=["config3-irs-band", "config3-ipm-band", "adaptive"],
                     help="profiler capture of one case: config3-irs-band = the rectangular Kroupa IRS configuration "
                          "(order 16, 64 rays per pixel) on 512 ray rows through the lattice centre, --steps runs; "
                          "adaptive = the learned-adaptive map (4096^2), --steps runs")
@@ -959,8 +959,9 @@ def main():
 
 def profile_case(args):
     """A small case for profiler captures (not a bench line): prints the
-    device time per run of the IRS lens-equation kernel, or of the adaptive
-    map's base and adaptive passes."""
+    device time per run of the IRS lens-equation kernel or of the IPM
+    deposition on a band of the rectangular Kroupa configuration, or of the
+    adaptive map's base and adaptive passes."""
     import irs_b200
     if args.case == "adaptive":
         a = irs_b200.AdaptiveIPM(tolerance=1e-3, audit_fraction=0.0025, audit_bound=0.05, **ADAPTIVE_CONFIG)
@@ -970,6 +971,21 @@ def profile_case(args):
                           "t_refine_deposit_ms": a.value("t_refine_deposit") * 1e3,
                           "cells_evaluated": a.value("cells_evaluated")}))
         a.close()
+        return
+    if args.case == "config3-ipm-band":  # the 512 lattice rows through the centre
+        m = irs_b200.IPM(**CONFIG3, num_rays_y=1, is_double=False)
+        m.derive()
+        ny = int(m.value("num_ray_threads_2"))
+        m.lib.set_band(m.obj, ny // 2 - 256, ny // 2 + 256)
+        m.run()
+        ts = []
+        for _ in range(max(1, args.steps)):
+            m.rerun(1)
+            ts.append(m.value("t_deposit"))
+        cells = int(m.value("num_ray_threads_1")) * 512
+        print(json.dumps({"case": args.case, "cells": cells, "deposit_ms": float(np.min(ts)) * 1e3,
+                          "cells_per_s": cells / float(np.min(ts))}))
+        m.close()
         return
     r = irs_b200.IRS(**CONFIG3, num_rays_y=64, is_double=False)
     r.derive()

@@ -62,6 +62,13 @@ struct RN<double> {
   }
 };
 
+// Fire-and-forget add to a map word in global memory (PTX red): the adding
+// thread never reads the word back, so no old value has to travel back to it
+// (a plain atomicAdd on these generic pointers compiles to a returning atom).
+__device__ __forceinline__ void red_add(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.global.add.u64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v) : "memory");
+}
+
 template <typename D>
 __device__ __forceinline__ D dabs(D a) {
   return a < D(0) ? -a : a;
@@ -350,8 +357,8 @@ __device__ __forceinline__ void deposit_row(const Tri<D>& t, int r, int npx, Dep
   if (xa < xb) {
     const unsigned long long q = RN<D>::to_fix(t.scale);
     const long long dbase = row * ((long long)npx + 1) + t.ox;
-    atomicAdd(M.diff + dbase + xa, q);
-    atomicAdd(M.diff + dbase + xb, (unsigned long long)(0ULL - q));
+    red_add(M.diff + dbase + xa, q);
+    red_add(M.diff + dbase + xb, (unsigned long long)(0ULL - q));
   }
   for (int c = cmin; c <= cmax; c++) {
     if (xa < xb && c == xa) {
@@ -361,7 +368,7 @@ __device__ __forceinline__ void deposit_row(const Tri<D>& t, int r, int npx, Dep
     D a = pixel_coverage(t, g, D(c), ht, ct0, ct1);
     if (a > D(0)) {
       unsigned long long q = RN<D>::to_fix(RN<D>::mul(a, t.scale));
-      if (q) atomicAdd(M.acc + rbase + c, q);
+      if (q) red_add(M.acc + rbase + c, q);
     }
   }
 }
@@ -486,7 +493,7 @@ __device__ __forceinline__ void deposit_warp_cells(const double2* __restrict__ v
       if (h.single && (starts >> lane & 1u)) {
         const unsigned later = starts & ~((2u << lane) - 1u);  // lane 31: mask of all bits, none later
         const int end = later ? __ffs(later) - 1 : 32;
-        atomicAdd(a, (unsigned long long)(end - lane) * RN<D>::to_fix(RN<D>::mul(factor, D(kFixScale))));
+        red_add(a, (unsigned long long)(end - lane) * RN<D>::to_fix(RN<D>::mul(factor, D(kFixScale))));
       }
     }
     const bool cx = h.nrows > 0 && !h.single;

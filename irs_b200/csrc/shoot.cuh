@@ -186,6 +186,12 @@ struct NearPairs {
   ulonglong2 coef[kMaxOrder];  // (re, re), (im, im)
 };
 
+// Fire-and-forget add of a ray count in global memory (PTX red; the count is
+// never read back by the adding thread).
+__device__ __forceinline__ void red_add_s32(int* p, int v) {
+  asm volatile("red.global.add.s32 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "r"(v) : "memory");
+}
+
 // Adds one ray count with the reference's clamp and row flip; (px, py) are the
 // source position in pixel units (unflipped).
 __device__ __forceinline__ void irs_deposit(double px, double py, int npx, int npy, int* __restrict__ pix,
@@ -195,8 +201,8 @@ __device__ __forceinline__ void irs_deposit(double px, double py, int npx, int n
   if (ix == npx) ix--;
   if (iy == npy) iy--;
   long long idx = (long long)(npy - 1 - iy) * npx + ix;
-  if (parities) atomicAdd(parity_min ? &pmin[idx] : &psad[idx], 1);
-  atomicAdd(&pix[idx], 1);
+  if (parities) red_add_s32(parity_min ? &pmin[idx] : &psad[idx], 1);
+  red_add_s32(&pix[idx], 1);
 }
 
 // ----------------------------------------------------------------- FP64 form
