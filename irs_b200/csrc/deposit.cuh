@@ -551,8 +551,10 @@ struct DepositPiece {
   int r;               // realization (map index)
 };
 
-// Batched deposition: the warps stride over the 32-cell chunks of all pieces
-// of the pass; a chunk's piece is found by a binary search over chunk0.
+// Batched deposition: the warps stride over blocks of 8 consecutive 32-cell
+// chunks of all pieces of the pass; a block's first piece is found by a
+// binary search over chunk0 and the next chunks advance from it (one search
+// per 8 chunks: 1.79 against 1.88 s for the 4096-pixel adaptive map).
 // Realization r accumulates into the maps at r * map_stride / r * diff_stride.
 template <typename D>
 __global__ void __launch_bounds__(kDepositThreads, sizeof(D) == 4 ? 16 : 8)
@@ -563,17 +565,22 @@ __global__ void __launch_bounds__(kDepositThreads, sizeof(D) == 4 ? 16 : 8)
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   __shared__ TriSlots<D> slots[kDepositWarps];
   TriSlots<D>& stage = slots[threadIdx.x >> 5];
-  for (long long g = warp0; g < nchunks; g += nwarps) {
-    int lo = 0, hi = npieces - 1;  // last piece with chunk0 <= g
+  constexpr int K = 8;  // consecutive chunks per visit: one piece search per K chunks
+  for (long long g0 = warp0 * K; g0 < nchunks; g0 += nwarps * K) {
+    int lo = 0, hi = npieces - 1;  // last piece with chunk0 <= g0
     while (lo < hi) {
       int mid = (lo + hi + 1) >> 1;
-      if (pieces[mid].chunk0 <= g) lo = mid;
+      if (pieces[mid].chunk0 <= g0) lo = mid;
       else hi = mid - 1;
     }
-    const DepositPiece<D> pc = pieces[lo];
-    const DepositMaps M{maps.acc + pc.r * map_stride, maps.diff + pc.r * diff_stride};
-    deposit_warp_cells<D>(verts + pc.voff, pc.ncx, pc.vstride, pc.ncx * pc.ncy, (g - pc.chunk0) * 32, pc.factor,
-                          npx, npy, M, M, M, 0, stage, pc.vstep, pc.ox, pc.oy, pc.inv_scale);
+    const long long gend = g0 + K < nchunks ? g0 + K : nchunks;
+    for (long long g = g0; g < gend; g++) {
+      while (lo + 1 < npieces && pieces[lo + 1].chunk0 <= g) lo++;
+      const DepositPiece<D> pc = pieces[lo];
+      const DepositMaps M{maps.acc + pc.r * map_stride, maps.diff + pc.r * diff_stride};
+      deposit_warp_cells<D>(verts + pc.voff, pc.ncx, pc.vstride, pc.ncx * pc.ncy, (g - pc.chunk0) * 32, pc.factor,
+                            npx, npy, M, M, M, 0, stage, pc.vstep, pc.ox, pc.oy, pc.inv_scale);
+    }
   }
 }
 
