@@ -22,9 +22,10 @@
 // Work distribution: a CTA takes one (leaf, 32x32 tile) work item at a time
 // (grid-stride over the global tile list), stages the leaf's <= 32 near stars
 // and <= 31 coefficients in shared memory, and every lane reads them as
-// warp-wide broadcasts. Each thread evaluates 4 lattice points (rows ty,
-// ty+8, ty+16, ty+24 of the tile) against each staged star, so one
-// shared-memory read feeds 4 evaluations. Without parities the FP32 form runs
+// warp-wide broadcasts. Each thread evaluates R lattice points (rows ty,
+// ty + 32/R, ... of the tile; R = 8, 4 or 2 at 128, 256 or 512 threads per
+// CTA) against each staged star, so one shared-memory read feeds R
+// evaluations. Without parities the FP32 form runs
 // its near and far field on pairs of points with the paired FP32 instructions
 // of sm_100 (near_far_pairs): half the issue slots, the same bits.
 //
