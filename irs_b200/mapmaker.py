@@ -14,6 +14,7 @@ formula), precision (0 = default form of the library, 1 = FP64 plain,
 from __future__ import annotations
 
 import ctypes as C
+import sys
 
 import numpy as np
 
@@ -480,7 +481,17 @@ class _MapMaker:
         # the map lands in a fresh numpy array during run(), chunk by chunk as
         # it arrives from the device
         pix_t = self.lib.get_pixels.restype._type_
-        out = np.empty((self.num_pixels_y2, self.num_pixels_y1), dtype=pix_t)
+        shape = (self.num_pixels_y2, self.num_pixels_y1)
+        out = getattr(self, "magnifications", None)
+        # the previous map's memory is reused when nothing outside this object
+        # refers to it (no caller variable or view: references here are the
+        # attribute, `out` and getrefcount's argument), so that a loop of runs
+        # does not fault fresh pages in for every map
+        if not (isinstance(out, np.ndarray) and out.shape == shape and out.dtype == np.dtype(pix_t)
+                and out.base is None and out.flags.c_contiguous and out.flags.writeable
+                and sys.getrefcount(out) <= 3):
+            out = np.empty(shape, dtype=pix_t)
+        self.magnifications = None
         self.lib.set_pixels_out(self.obj, out.ctypes.data_as(C.POINTER(pix_t)))
         ok = self.lib.run(self.obj, self.verbose)
         self.lib.set_pixels_out(self.obj, None)

@@ -50,6 +50,30 @@ def test_saved_files_read_back_through_util(gpu, tmp_path):
     assert hist.dtype == np.int32 and hist[:, 1].sum() == m.magnifications.size
 
 
+def test_run_never_overwrites_a_map_the_caller_holds(gpu):
+    """run() reuses the previous map's memory only when nothing outside the
+    object refers to it: a map the caller keeps (or a view of it) survives the
+    next run unchanged, and a map nobody keeps is refilled with the new one."""
+    m = irs_b200.IPM(**IPM_SMALL)
+    m.run()
+    kept = m.magnifications
+    snap = kept.copy()
+    view = m.magnifications[:4]
+    m.random_seed = 23
+    m.run()
+    assert m.magnifications is not kept
+    np.testing.assert_array_equal(kept, snap)
+    assert not np.array_equal(m.magnifications, snap)
+    del kept, view
+    other = m.magnifications.copy()
+    addr = m.magnifications.ctypes.data
+    m.random_seed = 22
+    m.run()
+    assert m.magnifications.ctypes.data == addr  # nobody held it: reused
+    np.testing.assert_array_equal(m.magnifications, snap)  # seed 22 again: the first map
+    assert not np.array_equal(m.magnifications, other)
+
+
 def test_star_generation_statistics(gpu):
     m = irs_b200.IPM(**IPM_SMALL, is_double=True)
     m.run()
