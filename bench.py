@@ -853,7 +853,7 @@ def our_arm(args):
         roof = {"kernel": "ipm_deposit_cells", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "traffic_unit": "GB per launch",
                 "traffic_source": "ncu on the 500^2 case (18.3 B per cell), scaled by cells",
-                "limiter": "instruction issue and latency (ncu, 500^2 case: 59 % issue-active, ALU pipe 45 %)",
+                "limiter": "instruction issue and latency (ncu, 500^2 case: 65 % issue-active, ALU pipe 51 %)",
                 "algorithmic": f"16 B x {nverts} corner positions + 8 B x {npix} map words"}
 
     # ---- secondary measurements (not the headline): the plain FP64 form of the
