@@ -848,11 +848,11 @@ def our_arm(args):
         achieved = bytes_ / (dep_ms * 1e-3) / 1e9
         peak = peaks.get("hbm_gbs", 6650.0)
         # DRAM traffic measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the 500^2 case of
-        # the same lens and pixel scale: 533 MB for 29.2 M cells, 18.3 B per cell, scaled to this launch
-        traffic = 18.3 * ncells / 1e9
+        # the same lens and pixel scale: 519 MB for 29.2 M cells, 17.8 B per cell, scaled to this launch
+        traffic = 17.8 * ncells / 1e9
         roof = {"kernel": "ipm_deposit_cells", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "traffic_unit": "GB per launch",
-                "traffic_source": "ncu on the 500^2 case (18.3 B per cell), scaled by cells",
+                "traffic_source": "ncu on the 500^2 case (17.8 B per cell), scaled by cells",
                 "limiter": "instruction issue and latency (ncu, 500^2 case: 65 % issue-active, ALU pipe 51 %)",
                 "algorithmic": f"16 B x {nverts} corner positions + 8 B x {npix} map words"}
 
