@@ -855,6 +855,12 @@ def our_arm(args):
                 "traffic_source": "ncu on the 500^2 case (17.8 B per cell), scaled by cells",
                 "limiter": "instruction issue and latency (ncu, 500^2 case: 65 % issue-active, ALU pipe 51 %)",
                 "algorithmic": f"16 B x {nverts} corner positions + 8 B x {npix} map words"}
+    # the lens-equation kernel against the FP32 FMA roofline, whichever kernel dominates
+    lens_tflops = flop_per_vertex * nverts / (lat_ms * 1e-3) / 1e12
+    roof_lens = {"kernel": "shoot_f32 (lattice lens equation)", "bound": "fp32", "achieved": lens_tflops,
+                 "peak": fp32_peak, "unit": "TFLOP/s", "frac": lens_tflops / fp32_peak, "ms": lat_ms,
+                 "peak_source": "148 SMs x 128 FP32 lanes x 2 x sm_max_mhz of MEASURED_PEAKS.json (derived)",
+                 "algorithmic": f"(11 x {near:.2f} near stars + 8 x {p} + 30) flop x {nverts} corners"}
 
     # ---- secondary measurements (not the headline): the plain FP64 form of the
     # same IPM workload, and IRS on the plain-IRS case in both forms
@@ -878,6 +884,10 @@ def our_arm(args):
             extra[key] = {"rays_per_s": rays / float(np.mean(ts)), "rays": int(rays), "stars": int(r.num_stars),
                           "ms_per_step": float(np.mean(ts)) * 1e3, "shoot_ms": r.value("t_lattice") * 1e3,
                           "rays_received": int(r.num_rays_received)}
+            if not dbl:  # the lens kernel against the FP32 FMA roofline (flop per ray as for a lattice corner)
+                fl = (11 * r.value("mean_near") + 8 * r.expansion_order + 30) * rays / (r.value("t_lattice") * 1e12)
+                extra[key]["lens_tflops"] = fl
+                extra[key]["lens_frac_of_fp32_peak"] = fl / fp32_peak
             r.close()
         # the workload's lens through the graph-captured pipeline (one realization, the
         # library's own star field of the workload's seed), against the same realization run singly
@@ -920,6 +930,7 @@ def our_arm(args):
             "e2e": {"value": ws * args.steps * npix / e2e_time, "unit": "pixels/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "roofline": roof,
+            "roofline_lens": roof_lens,
             "kernels_ms": {"lattice": lat_ms, "deposit": dep_ms, "pipeline": dev_time / args.steps * 1e3},
             "mean_near_stars": near,
             "gpu_launches": launches,
